@@ -1,0 +1,132 @@
+/* spdk.h - C ABI of the spd_K B200 solver (libspdk_cuda.so).
+ *
+ * Plain C types only: a caller binds these with ctypes, cgo, JNI or a C++
+ * host exactly as it would the reference's C++ entry points. All device
+ * buffers are owned by the library; host buffers are owned by the caller.
+ * Every function returns 0 on success, a negative SPDK_E* code on a usage
+ * or CUDA error, and a positive code for a device-detected numerical fault.
+ * spdk_last_error() gives the message of the last failure on this thread.
+ *
+ * Correspondence with the reference (paths inside davidvelasco07/spd_K):
+ *   spdk_hydro_config      RunConfig + ProblemParams + <mesh> (src/global.hpp:20-60,
+ *                          src/main.cpp:126-189)
+ *   spdk_hydro_create      Hydro_ader::Hydro_ader (src/hydro_ader.hpp:76-213)
+ *   spdk_hydro_step        one pass of the loop body of Hydro_ader::time_evolution
+ *                          (src/hydro_ader.hpp:234-243): ADER_step (:291-305) or
+ *                          RK_step (:313-325), compute_primitives, transform_sp_to_cv,
+ *                          compute_dt
+ *   spdk_hydro_evolve      Hydro_ader::time_evolution (src/hydro_ader.hpp:215-273)
+ *   spdk_hydro_get_dt      compute_dt result (src/hydro.cpp:208-262)
+ */
+#ifndef SPDK_H
+#define SPDK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPDK_ABI_VERSION 1
+
+enum {
+    SPDK_OK = 0,
+    SPDK_E_ARG = -1,       /* invalid argument / unsupported configuration */
+    SPDK_E_CUDA = -2,      /* CUDA runtime error (message in spdk_last_error) */
+    SPDK_E_NOMEM = -3,     /* device allocation failed */
+    SPDK_E_STATE = -4      /* call out of order */
+};
+
+enum { SPDK_BC_PERIODIC = 0, SPDK_BC_GRADFREE = 1, SPDK_BC_REFLECTIVE = 2 };
+enum { SPDK_INTEGRATOR_ADER = 0, SPDK_INTEGRATOR_RK = 1 };
+
+/* initial conditions: 0-9 are the reference's (src/define.hpp:58-60),
+ * 10-12 are project problems without a reference counterpart */
+enum {
+    SPDK_IC_SINE_WAVE = 0, SPDK_IC_SEDOV = 1, SPDK_IC_SPHERICAL_BLAST = 2,
+    SPDK_IC_SQUARE = 3, SPDK_IC_SOD = 4, SPDK_IC_SHU_OSHER = 5,
+    SPDK_IC_KELVIN_HELMHOLTZ = 6, SPDK_IC_IMPLOSION = 7, SPDK_IC_RTI = 8,
+    SPDK_IC_USER = 9, SPDK_IC_KH_NOISE = 10, SPDK_IC_QUADRANT = 11,
+    SPDK_IC_RTI_TOP = 12
+};
+
+/* arithmetic of the solver */
+enum {
+    SPDK_PRECISION_FP64 = 0   /* plain form: FP64, reference operation order */
+};
+
+typedef struct spdk_hydro_config {
+    int p;                 /* polynomial degree, 1..7 */
+    int N[3];              /* elements per direction; N=1 marks an inactive direction */
+    double L[3];           /* box lengths */
+    int bc[3];             /* SPDK_BC_* per direction */
+    int integrator;        /* SPDK_INTEGRATOR_* */
+    int rk_order;          /* 1, 2 or 3 (SSP-RK) */
+    int fallback;          /* a-posteriori NAD + MUSCL-Hancock fallback */
+    double gamma, cfl;
+    double g[3];           /* constant gravitational acceleration */
+    double nad_tolerance;
+    int nad_delta, nad_moore, sed, blending;
+    int problem;           /* SPDK_IC_* */
+    double amp, v1, v2, v3, d0, d1, p0, p1, radius, sigma;
+    int dir;
+    double cx, cy, cz;
+    double q[16];          /* extra parameters of project problems */
+    unsigned long long seed;
+    int precision;         /* SPDK_PRECISION_* */
+    int device;            /* CUDA device ordinal */
+} spdk_hydro_config;
+
+typedef struct spdk_hydro spdk_hydro;
+
+typedef struct spdk_hydro_info {
+    int ndim, p, n_points, nvar;  /* points per element, conserved slots (ndim+2) */
+    int N[3];
+    long long n_elements;
+    long long n_dof;              /* active solution points */
+    int n_time_slices;            /* p+1 (ADER) or 1 (RK) */
+    int launches_per_step;        /* kernels launched by one spdk_hydro_step */
+    size_t device_bytes;          /* device memory held by the solver */
+} spdk_hydro_info;
+
+/* fields for spdk_hydro_read / spdk_hydro_write; layout [element][var][point]
+ * with element = (k*N[1] + j)*N[0] + i over active elements and
+ * point = (kk*n + jj)*n + ii, n = p+1 */
+enum {
+    SPDK_FIELD_U_SP = 0,      /* conserved state at solution points */
+    SPDK_FIELD_W_CV = 1,      /* primitive sub-cell averages (written every step) */
+    SPDK_FIELD_TROUBLES = 2,  /* last fallback slice's trouble flags, 0/1 per sub-cell */
+    SPDK_FIELD_THETA = 3      /* last fallback slice's blending factor per sub-cell */
+};
+
+const char* spdk_last_error(void);
+int spdk_abi_version(void);
+
+int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out);
+int spdk_hydro_destroy(spdk_hydro* h);
+int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info);
+
+/* time step for the next spdk_hydro_step (blocks on the solver stream) */
+int spdk_hydro_get_dt(spdk_hydro* h, double* dt);
+/* impose the next dt (the reference's output clamping) */
+int spdk_hydro_set_dt(spdk_hydro* h, double dt);
+/* one step with the current dt; the next dt is reduced on the device.
+ * Asynchronous with respect to the host. */
+int spdk_hydro_step(spdk_hydro* h);
+/* n steps, each with the dt its predecessor computed, replayed from a CUDA
+ * graph; asynchronous */
+int spdk_hydro_steps(spdk_hydro* h, int n);
+/* time_evolution: steps until t >= t_end; dt_output > 0 clamps dt to hit
+ * output times exactly. Returns the number of steps and the final t. */
+int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t);
+int spdk_hydro_sync(spdk_hydro* h);
+/* copy a field to / from host memory (count = number of doubles); writing
+ * SPDK_FIELD_U_SP recomputes W_cv and dt */
+int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count);
+int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPDK_H */

@@ -1,0 +1,610 @@
+// spd_K B200 hydro solver: device state, step orchestration and the C ABI
+// declared in include/spdk.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "spdk.h"
+#include "spdk_fallback.cuh"
+#include "spdk_kernels.cuh"
+#include "spdk_setup.h"
+
+namespace spdk {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define SPDK_CUDA(call)                                                                  \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(SPDK_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// element-local set-up kernels
+// ---------------------------------------------------------------------------
+// U_sp = conservatives(cv_to_sp(W_cv)) and dt(W_cv): the constructor tail
+// (src/hydro_ader.hpp:205-208)
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads) init_state_kernel(DevGrid G, DevMats M, const double* __restrict__ wcv,
+                                                             double* __restrict__ u,
+                                                             unsigned long long* dtmin) {
+    using S = Shape<D, P>;
+    constexpr int V = S::V, NPT = S::NPT;
+    __shared__ double b0[V * NPT], b1[V * NPT];
+    const long long ge = blockIdx.x;
+    for (int q = threadIdx.x; q < V * NPT; q += blockDim.x) b0[q] = wcv[ge * V * NPT + q];
+    __syncthreads();
+    double dtl = 1.7976931348623157e308;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V];
+        for (int v = 0; v < V; v++) w[v] = b0[v * NPT + q];
+        dtl = smin(dtl, point_dt<D>(G, w, S::n));
+    }
+    double* bufs[2] = {b1, b0};
+    const double* src = b0;
+    for (int d = 0; d < D; d++) {
+        double* dst = bufs[d % 2];
+        sweep_smem<D, P>(src, dst, M.cv_to_sp, d, V * NPT);
+        __syncthreads();
+        src = dst;
+    }
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V], uu[V];
+        for (int v = 0; v < V; v++) w[v] = src[v * NPT + q];
+        conservatives<D>(w, uu, G.gm);
+        for (int v = 0; v < V; v++) u[ge * V * NPT + v * NPT + q] = uu[v];
+    }
+    block_min_dt(dtl, dtmin);
+}
+
+// W_cv = sp_to_cv(primitives(U_sp)) and dt, for a state written by the host
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMats M, const double* __restrict__ u,
+                                                         double* __restrict__ wcv, unsigned long long* dtmin) {
+    using S = Shape<D, P>;
+    constexpr int V = S::V, NPT = S::NPT;
+    __shared__ double b0[V * NPT], b1[V * NPT];
+    const long long ge = blockIdx.x;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double uu[V], w[V];
+        for (int v = 0; v < V; v++) uu[v] = u[ge * V * NPT + v * NPT + q];
+        primitives<D>(uu, w, G.gm);
+        for (int v = 0; v < V; v++) b0[v * NPT + q] = w[v];
+    }
+    __syncthreads();
+    double* bufs[2] = {b1, b0};
+    const double* src = b0;
+    for (int d = 0; d < D; d++) {
+        double* dst = bufs[d % 2];
+        sweep_smem<D, P>(src, dst, M.sp_to_cv, d, V * NPT);
+        __syncthreads();
+        src = dst;
+    }
+    double dtl = 1.7976931348623157e308;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V];
+        for (int v = 0; v < V; v++) {
+            w[v] = src[v * NPT + q];
+            wcv[ge * V * NPT + v * NPT + q] = w[v];
+        }
+        dtl = smin(dtl, point_dt<D>(G, w, S::n));
+    }
+    block_min_dt(dtl, dtmin);
+}
+
+// next dt <- reduced minimum; re-arm the reduction
+__global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin) {
+    *dt = __longlong_as_double((long long)*dtmin);
+    *dtmin = 0x7FEFFFFFFFFFFFFFULL;
+}
+
+// ---------------------------------------------------------------------------
+// kernel table of one (D, P, tile) instantiation
+// ---------------------------------------------------------------------------
+struct KernelSet {
+    void (*predict)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*correct)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*flux)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*detect)(DevGrid, const double2*, const double2*, uint8_t*, int*) = nullptr;
+    void (*theta)(DevGrid, const uint8_t*, uint8_t*) = nullptr;
+    void (*update)(DevGrid, DevMats, FallbackArgs) = nullptr;
+    void (*init)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
+    void (*derive)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
+    size_t picard_smem = 0, update_smem = 0;
+    int tile[3] = {1, 1, 1};
+};
+
+template <int D, int P, int TX, int TY, int TZ>
+KernelSet make_set() {
+    KernelSet k;
+    k.predict = picard_kernel<D, P, TX, TY, TZ, kPredict>;
+    k.correct = picard_kernel<D, P, TX, TY, TZ, kCorrect>;
+    k.flux = picard_kernel<D, P, TX, TY, TZ, kFlux>;
+    k.detect = fv_detect_kernel<D, P>;
+    k.theta = fv_theta_kernel<D, P, TX, TY, TZ>;
+    k.update = fv_update_kernel<D, P, TX, TY, TZ>;
+    k.init = init_state_kernel<D, P>;
+    k.derive = derive_kernel<D, P>;
+    k.picard_smem = picard_smem_bytes<D, P, TX, TY, TZ>();
+    k.update_smem = UpdateSmem<D, P, TX, TY, TZ>::bytes;
+    k.tile[0] = TX;
+    k.tile[1] = TY;
+    k.tile[2] = TZ;
+    return k;
+}
+
+// Tile choice: the largest instantiated tile that divides the element counts.
+template <int P>
+bool pick2(int Nx, int Ny, KernelSet* k) {
+    if (P <= 4 && Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
+    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<2, P, 2, 2, 1>(); return true; }
+    *k = make_set<2, P, 1, 1, 1>();
+    return true;
+}
+template <int P>
+bool pick3(int, int, int, KernelSet* k) {
+    *k = make_set<3, P, 1, 1, 1>();
+    return true;
+}
+
+bool select_kernels(int D, int p, const int N[3], KernelSet* k) {
+    if (D == 2) {
+        switch (p) {
+        case 1: return pick2<1>(N[0], N[1], k);
+        case 2: return pick2<2>(N[0], N[1], k);
+        case 3: return pick2<3>(N[0], N[1], k);
+        case 4: return pick2<4>(N[0], N[1], k);
+        case 5: return pick2<5>(N[0], N[1], k);
+        case 6: return pick2<6>(N[0], N[1], k);
+        case 7: return pick2<7>(N[0], N[1], k);
+        }
+    } else if (D == 3) {
+        switch (p) {
+        case 1: return pick3<1>(N[0], N[1], N[2], k);
+        case 2: return pick3<2>(N[0], N[1], N[2], k);
+        case 3: return pick3<3>(N[0], N[1], N[2], k);
+        case 4: return pick3<4>(N[0], N[1], N[2], k);
+        case 5: return pick3<5>(N[0], N[1], N[2], k);
+        }
+    }
+    return false;
+}
+
+}  // namespace spdk
+
+using namespace spdk;
+
+struct spdk_hydro {
+    spdk_hydro_config cfg{};
+    int D = 2, p = 3, n = 4, nf = 5, V = 4, NPT = 16, nt = 4, nstages = 1;
+    double rk_a[3] = {0, 0, 0};
+    long long E = 0;
+    Matrices mats;
+    Axis ax[3];
+    DevMats dm{};
+    DevGrid G{};
+    KernelSet ks;
+    cudaStream_t stream = nullptr;
+    double *u = nullptr, *ua[2] = {nullptr, nullptr}, *u0 = nullptr, *ucv[2] = {nullptr, nullptr};
+    double *ff[3] = {nullptr, nullptr, nullptr}, *wcv = nullptr, *dt = nullptr;
+    double *fvf[3] = {nullptr, nullptr, nullptr}, *fvc[3] = {nullptr, nullptr, nullptr};
+    double2 *rpo = nullptr, *rpn = nullptr;
+    uint8_t *trouble = nullptr, *theta = nullptr;
+    unsigned long long* dtmin = nullptr;
+    size_t bytes = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int launches = 0;
+};
+
+namespace {
+
+int dalloc(spdk_hydro* h, void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess)
+        return fail(SPDK_E_NOMEM, "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    h->bytes += bytes;
+    return 0;
+}
+
+unsigned grid_blocks(const spdk_hydro* h) {
+    long long b = 1;
+    for (int d = 0; d < h->D; d++) b *= h->G.N[d] / h->ks.tile[d];
+    return (unsigned)b;
+}
+
+// launches of one step, recorded on h->stream (also used for capture)
+int enqueue_step(spdk_hydro* h) {
+    const KernelSet& k = h->ks;
+    const unsigned blocks = grid_blocks(h);
+    const unsigned cells_blocks = (unsigned)((h->E * h->NPT + kThreads - 1) / kThreads);
+    int launches = 0;
+    if (h->nstages > 1)
+        SPDK_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)h->E * h->V * h->NPT * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, h->stream));
+    for (int s = 0; s < h->nstages; s++) {
+        const bool final_stage = s == h->nstages - 1;
+        PicardArgs A{};
+        A.u = h->u;
+        A.dt = h->dt;
+        const double* in = h->u;
+        int in_slices = 1;
+        // Picard predictor passes (ADER only: nt = p+1)
+        for (int it = 0; it + 1 < h->nt; it++) {
+            A.ua_in = in;
+            A.in_slices = in_slices;
+            A.ua_out = h->ua[it % 2];
+            k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            launches++;
+            in = h->ua[it % 2];
+            in_slices = h->nt;
+        }
+        A.ua_in = in;
+        A.in_slices = in_slices;
+        if (!h->cfg.fallback) {
+            A.u_out = h->u;
+            A.u0 = h->u0;
+            A.rk_a = h->rk_a[s];
+            A.final_stage = final_stage;
+            A.wcv = h->wcv;
+            A.dtmin = h->dtmin;
+            k.correct<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            launches++;
+        } else {
+            for (int d = 0; d < 3; d++) A.ff[d] = h->ff[d];
+            A.ucv = h->ucv[0];
+            A.rp_old = h->rpo;
+            A.rp_new = h->rpn;
+            k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            launches++;
+            for (int t = 0; t < h->nt; t++) {
+                k.detect<<<cells_blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
+                k.theta<<<blocks, kThreads, 0, h->stream>>>(h->G, h->trouble, h->theta);
+                FallbackArgs F{};
+                F.ucv_in = h->ucv[t % 2];
+                F.ucv_out = h->ucv[(t + 1) % 2];
+                F.ff0 = h->ff[0];
+                F.ff1 = h->ff[1];
+                F.ff2 = h->ff[2];
+                F.rp_old = h->rpo;
+                F.rp_new = h->rpn;
+                F.rp_old_next = h->rpo;
+                F.rp_new_next = h->rpn;
+                F.trouble = h->trouble;
+                F.theta = h->theta;
+                F.t = t;
+                F.last = t == h->nt - 1;
+                F.u = h->u;
+                F.u0 = h->u0;
+                F.rk_a = h->rk_a[s];
+                F.final_stage = final_stage;
+                F.wcv = h->wcv;
+                F.dtmin = h->dtmin;
+                F.dt = h->dt;
+                k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, h->dm, F);
+                launches += 3;
+            }
+        }
+    }
+    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+    launches++;
+    h->launches = launches;
+    SPDK_CUDA(cudaGetLastError());
+    return 0;
+}
+
+void release(spdk_hydro* h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
+                    h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
+                    h->rpo, h->rpn, h->trouble, h->theta, h->dtmin};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* spdk_last_error(void) { return spdk::g_last_error.c_str(); }
+int spdk_abi_version(void) { return SPDK_ABI_VERSION; }
+
+int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
+    if (!cfg || !out) return fail(SPDK_E_ARG, "null argument");
+    *out = nullptr;
+    const spdk_hydro_config& c = *cfg;
+    if (c.p < 1 || c.p > kMaxP) return fail(SPDK_E_ARG, "p must be in 1..7");
+    if (c.N[0] < 2 || c.N[1] < 2) return fail(SPDK_E_ARG, "x and y must be active (nx1, nx2 > 1)");
+    const int D = c.N[2] > 1 ? 3 : 2;
+    if (D == 3 && c.p > 5) return fail(SPDK_E_ARG, "3D runs support p <= 5");
+    if (D == 2 && (c.g[2] != 0.0 || ((c.problem == SPDK_IC_SINE_WAVE || c.problem == SPDK_IC_SQUARE) && c.v3 != 0.0)))
+        return fail(SPDK_E_ARG, "a 2D run cannot carry z momentum or z gravity");
+    if (c.precision != SPDK_PRECISION_FP64) return fail(SPDK_E_ARG, "unsupported precision");
+    for (int d = 0; d < D; d++)
+        if (c.bc[d] < 0 || c.bc[d] > 2) return fail(SPDK_E_ARG, "bad boundary type");
+    if (c.integrator == SPDK_INTEGRATOR_RK && (c.rk_order < 1 || c.rk_order > 3))
+        return fail(SPDK_E_ARG, "rk_order must be 1, 2 or 3");
+
+    spdk_hydro* h = new spdk_hydro();
+    h->cfg = c;
+    h->D = D;
+    h->p = c.p;
+    h->n = c.p + 1;
+    h->nf = c.p + 2;
+    h->V = D + 2;
+    h->NPT = D == 2 ? h->n * h->n : h->n * h->n * h->n;
+    const bool ader = c.integrator == SPDK_INTEGRATOR_ADER;
+    h->nt = ader ? c.p + 1 : 1;
+    h->nstages = 1;
+    if (!ader) {
+        h->nstages = c.rk_order;
+        if (c.rk_order == 2) h->rk_a[1] = 0.5;
+        if (c.rk_order == 3) { h->rk_a[1] = 0.75; h->rk_a[2] = 1.0 / 3.0; }
+    }
+    int N[3] = {c.N[0], c.N[1], D == 3 ? c.N[2] : 1};
+    if (!select_kernels(D, c.p, N, &h->ks)) {
+        delete h;
+        return fail(SPDK_E_ARG, "no kernel instantiation for this ndim/p");
+    }
+    int rc = cudaSetDevice(c.device) == cudaSuccess ? 0 : fail(SPDK_E_CUDA, "cudaSetDevice failed");
+    if (rc) { delete h; return rc; }
+    build_matrices(c.p, ader, &h->mats);
+    for (int d = 0; d < 3; d++) build_axis(N[d], c.p, c.L[d], h->mats.x_fp, d < D, &h->ax[d]);
+    // device matrices (same values as the host setup)
+    const int n = h->n, nf = h->nf;
+    std::memset(&h->dm, 0, sizeof(h->dm));
+    for (int j = 0; j < nf; j++)
+        for (int i = 0; i < n; i++) h->dm.sp_to_fp[j * n + i] = h->mats.sp_to_fp[j * n + i];
+    for (int j = 0; j < n; j++)
+        for (int i = 0; i < nf; i++) h->dm.dfp_to_sp[j * nf + i] = h->mats.dfp_to_sp[j * nf + i];
+    for (int q = 0; q < n * n; q++) {
+        h->dm.sp_to_cv[q] = h->mats.sp_to_cv[q];
+        h->dm.cv_to_sp[q] = h->mats.cv_to_sp[q];
+    }
+    for (int q = 0; q < h->nt * h->nt; q++) h->dm.invader[q] = h->mats.invader[q];
+    for (int q = 0; q < h->nt; q++) h->dm.wt[q] = h->mats.wt[q];
+    // grid
+    DevGrid& G = h->G;
+    h->E = (long long)N[0] * N[1] * N[2];
+    for (int d = 0; d < 3; d++) {
+        G.N[d] = N[d];
+        G.bc[d] = c.bc[d];
+        G.h[d] = h->ax[d].h;
+        int ex = 0;
+        const double m = std::frexp(G.h[d], &ex);
+        G.pow2[d] = (m == 0.5) ? 1 : 0;
+        G.rh[d] = G.pow2[d] ? std::ldexp(1.0, 1 - ex) : 0.0;
+        G.g[d] = c.g[d];
+    }
+    G.gm = c.gamma;
+    G.cfl = c.cfl;
+    G.grav = (c.g[0] != 0.0 || c.g[1] != 0.0 || c.g[2] != 0.0) ? 1 : 0;
+    G.nt = h->nt;
+    G.E = h->E;
+    G.nad_tol = c.nad_tolerance;
+    G.nad_delta = c.nad_delta;
+    G.nad_moore = c.nad_moore;
+    G.use_sed = (c.sed && c.p > 1) ? 1 : 0;
+    G.blending = c.blending;
+
+    const size_t state = (size_t)h->E * h->V * h->NPT * sizeof(double);
+    rc = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess
+             ? 0 : fail(SPDK_E_CUDA, "cudaStreamCreate failed");
+    if (!rc) rc = dalloc(h, (void**)&h->u, state);
+    if (!rc && h->nt > 1) {
+        rc = dalloc(h, (void**)&h->ua[0], state * h->nt);
+        if (!rc) rc = dalloc(h, (void**)&h->ua[1], state * h->nt);
+    }
+    if (!rc && h->nstages > 1) rc = dalloc(h, (void**)&h->u0, state);
+    if (!rc) rc = dalloc(h, (void**)&h->wcv, state);
+    if (!rc) rc = dalloc(h, (void**)&h->dt, sizeof(double) * 2);
+    if (!rc) rc = dalloc(h, (void**)&h->dtmin, sizeof(unsigned long long));
+    if (!rc && c.fallback) {
+        const size_t ffb = (size_t)h->nt * h->E * h->V * (h->NPT / h->n) * h->nf * sizeof(double);
+        for (int d = 0; d < D && !rc; d++) rc = dalloc(h, (void**)&h->ff[d], ffb);
+        if (!rc) rc = dalloc(h, (void**)&h->ucv[0], state);
+        if (!rc) rc = dalloc(h, (void**)&h->ucv[1], state);
+        if (!rc) rc = dalloc(h, (void**)&h->rpo, (size_t)h->E * h->NPT * sizeof(double2));
+        if (!rc) rc = dalloc(h, (void**)&h->rpn, (size_t)h->E * h->NPT * sizeof(double2));
+        if (!rc) rc = dalloc(h, (void**)&h->trouble, (size_t)h->E * h->NPT);
+        if (!rc) rc = dalloc(h, (void**)&h->theta, (size_t)h->E * h->NPT);
+        for (int d = 0; d < D && !rc; d++) {
+            rc = dalloc(h, (void**)&h->fvf[d], h->ax[d].fv_faces.size() * sizeof(double));
+            if (!rc) rc = dalloc(h, (void**)&h->fvc[d], h->ax[d].fv_centers.size() * sizeof(double));
+            if (!rc && cudaMemcpy(h->fvf[d], h->ax[d].fv_faces.data(), h->ax[d].fv_faces.size() * sizeof(double),
+                                  cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = fail(SPDK_E_CUDA, "upload fv_faces");
+            if (!rc && cudaMemcpy(h->fvc[d], h->ax[d].fv_centers.data(),
+                                  h->ax[d].fv_centers.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+                rc = fail(SPDK_E_CUDA, "upload fv_centers");
+            G.fvf[d] = h->fvf[d];
+            G.fvc[d] = h->fvc[d];
+        }
+        if (!rc && cudaMemset(h->trouble, 0, (size_t)h->E * h->NPT) != cudaSuccess)
+            rc = fail(SPDK_E_CUDA, "memset");
+        if (!rc && cudaMemset(h->theta, 0, (size_t)h->E * h->NPT) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset");
+    }
+    if (!rc) {
+        const void* fns[] = {(const void*)h->ks.predict, (const void*)h->ks.correct, (const void*)h->ks.flux};
+        for (const void* f : fns)
+            if (!rc && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)h->ks.picard_smem) != cudaSuccess)
+                rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.picard_smem) + " bytes");
+        if (!rc && cudaFuncSetAttribute((const void*)h->ks.update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)h->ks.update_smem) != cudaSuccess)
+            rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.update_smem) + " bytes");
+    }
+    if (!rc) {
+        // initial condition on the host (transcendentals through the same libm as the reference)
+        std::vector<double> w0;
+        initial_wcv(c, h->mats, h->ax, D, &w0);
+        if (cudaMemcpy(h->wcv, w0.data(), state, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(SPDK_E_CUDA, "upload W_cv");
+    }
+    if (!rc) {
+        const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+        cudaMemcpy(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice);
+        h->ks.init<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm, h->wcv, h->u, h->dtmin);
+        advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+        cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = fail(SPDK_E_CUDA, std::string("init: ") + cudaGetErrorString(e));
+    }
+    if (rc) {
+        release(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+int spdk_hydro_destroy(spdk_hydro* h) {
+    if (!h) return 0;
+    cudaStreamSynchronize(h->stream);
+    release(h);
+    delete h;
+    return 0;
+}
+
+int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info) {
+    if (!h || !info) return fail(SPDK_E_ARG, "null argument");
+    info->ndim = h->D;
+    info->p = h->p;
+    info->n_points = h->NPT;
+    info->nvar = h->V;
+    for (int d = 0; d < 3; d++) info->N[d] = h->G.N[d];
+    info->n_elements = h->E;
+    info->n_dof = h->E * h->NPT;
+    info->n_time_slices = h->nt;
+    int l = 0;
+    for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 3 * h->nt : 1);
+    info->launches_per_step = l + 1;
+    info->device_bytes = h->bytes;
+    return 0;
+}
+
+int spdk_hydro_get_dt(spdk_hydro* h, double* dt) {
+    if (!h || !dt) return fail(SPDK_E_ARG, "null argument");
+    SPDK_CUDA(cudaMemcpyAsync(dt, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int spdk_hydro_set_dt(spdk_hydro* h, double dt) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    SPDK_CUDA(cudaMemcpyAsync(h->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int spdk_hydro_step(spdk_hydro* h) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    return enqueue_step(h);
+}
+
+int spdk_hydro_steps(spdk_hydro* h, int nsteps) {
+    if (!h || nsteps < 0) return fail(SPDK_E_ARG, "bad argument");
+    if (nsteps == 0) return 0;
+    if (!h->graph) {
+        // capture one step; replays reuse the same device pointers
+        cudaGraph_t g;
+        SPDK_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    }
+    for (int s = 0; s < nsteps; s++) SPDK_CUDA(cudaGraphLaunch(h->graph, h->stream));
+    return 0;
+}
+
+int spdk_hydro_sync(spdk_hydro* h) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t_out) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    // src/hydro_ader.hpp:215-273 with a blocking dt read per step, as there
+    double t = 0, dt = 0;
+    long long ns = 0;
+    int rc = spdk_hydro_get_dt(h, &dt);
+    if (rc) return rc;
+    const bool outputs = dt_output > 0;
+    double t_output = dt_output;
+    while (t < t_end) {
+        rc = enqueue_step(h);
+        if (rc) return rc;
+        t += dt;
+        ns++;
+        rc = spdk_hydro_get_dt(h, &dt);
+        if (rc) return rc;
+        if (outputs) {
+            if (t >= t_output) t_output = t + dt_output;
+            if (t + dt > t_output) {
+                dt = t_output - t;
+                rc = spdk_hydro_set_dt(h, dt);
+                if (rc) return rc;
+            }
+        }
+    }
+    if (steps) *steps = ns;
+    if (t_out) *t_out = t;
+    return 0;
+}
+
+int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count) {
+    if (!h || !host) return fail(SPDK_E_ARG, "null argument");
+    const size_t state = (size_t)h->E * h->V * h->NPT;
+    const size_t cells = (size_t)h->E * h->NPT;
+    if (field == SPDK_FIELD_U_SP || field == SPDK_FIELD_W_CV) {
+        if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
+        SPDK_CUDA(cudaMemcpyAsync(host, field == SPDK_FIELD_U_SP ? h->u : h->wcv, state * sizeof(double),
+                                  cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaStreamSynchronize(h->stream));
+        return 0;
+    }
+    if (field == SPDK_FIELD_TROUBLES || field == SPDK_FIELD_THETA) {
+        if (!h->cfg.fallback) return fail(SPDK_E_STATE, "fallback is off");
+        if (count != cells) return fail(SPDK_E_ARG, "count must be E*NPT = " + std::to_string(cells));
+        std::vector<uint8_t> b(cells);
+        SPDK_CUDA(cudaMemcpyAsync(b.data(), field == SPDK_FIELD_TROUBLES ? h->trouble : h->theta, cells,
+                                  cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaStreamSynchronize(h->stream));
+        for (size_t q = 0; q < cells; q++) host[q] = field == SPDK_FIELD_TROUBLES ? b[q] : b[q] * 0.125;
+        return 0;
+    }
+    return fail(SPDK_E_ARG, "unknown field");
+}
+
+int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count) {
+    if (!h || !host) return fail(SPDK_E_ARG, "null argument");
+    const size_t state = (size_t)h->E * h->V * h->NPT;
+    if (field != SPDK_FIELD_U_SP) return fail(SPDK_E_ARG, "only U_sp can be written");
+    if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
+    SPDK_CUDA(cudaMemcpyAsync(h->u, host, state * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+    SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
+    h->ks.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm, h->u, h->wcv, h->dtmin);
+    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+    SPDK_CUDA(cudaGetLastError());
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,711 @@
+// Fused device kernels of the spd_K B200 hydro step.
+//
+// State layout (device, FP64, no ghost elements):
+//   U, U_cv          [element][var][point]            V = D+2 slots
+//   U_ader (A and B) [slice][element][var][point]     ping-pong per Picard pass
+//   FF_d             [slice][element][var][face point] FV face fluxes of direction d,
+//                                                      laid out like the element's
+//                                                      d-flux points (n_f per line)
+//   RP_old, RP_new   [element][point] double2          (rho, p) of the FV candidate
+//   T, theta         [element][point] uint8            trouble flag / theta*8
+// element = (k*Ny + j)*Nx + i, point = (kk*n + jj)*n + ii.
+//
+// Boundary conditions are applied by index mapping instead of ghost storage:
+// an SD face on the domain edge pairs the element's own interface state with
+// its periodic partner, a copy (gradfree) or a mirror (reflective); FV ghost
+// cells are images of active cells (spdk::fv_image).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "spdk_physics.cuh"
+
+namespace spdk {
+
+constexpr int kThreads = 256;
+constexpr int kMaxNd = 8;    // n = p+1 <= 8
+constexpr int kMaxNfd = 9;
+
+// Transform matrices, passed by value (kernel parameter space)
+struct DevMats {
+    double sp_to_fp[kMaxNfd * kMaxNd];   // [nf][n]
+    double dfp_to_sp[kMaxNd * kMaxNfd];  // [n][nf]
+    double sp_to_cv[kMaxNd * kMaxNd];    // [n][n]
+    double cv_to_sp[kMaxNd * kMaxNd];
+    double invader[kMaxNd * kMaxNd];     // [nt][nt]
+    double wt[kMaxNd];
+};
+
+struct DevGrid {
+    int N[3];
+    int bc[3];
+    double h[3], rh[3];
+    int pow2[3];
+    double gm, cfl;
+    double g[3];
+    int grav;
+    int nt;
+    long long E;
+    const double* fvf[3];  // FV faces in frame indexing (active cell a has faces a+2, a+3)
+    const double* fvc[3];  // FV centres in frame indexing
+    // fallback settings
+    double nad_tol;
+    int nad_delta, nad_moore, use_sed, blending;
+};
+
+enum { kPredict = 0, kCorrect = 1, kFlux = 2 };
+
+struct PicardArgs {
+    const double* ua_in;   // [slice][E][V][NPT], or U when in_slices == 1
+    int in_slices;         // 1: every slice equals U (first Picard pass / RK stage)
+    const double* u;       // U_sp
+    double* ua_out;        // kPredict output
+    double* u_out;         // kCorrect output (may alias u: element-local)
+    const double* u0;      // RK step-start state
+    double rk_a;           // RK convex weight (0: none)
+    double* ff[3];         // kFlux: FV face fluxes, all slices
+    double* ucv;           // kFlux: U_cv = sp_to_cv(U)
+    double2* rp_old;       // kFlux: slice-0 candidate (rho, p) of U_old
+    double2* rp_new;       // kFlux: slice-0 candidate (rho, p) of U_new
+    double* wcv;           // kCorrect: W_cv output (nullable)
+    unsigned long long* dtmin;  // kCorrect: next-dt reduction
+    int final_stage;       // kCorrect: compute W_cv and dt
+    const double* dt;      // device dt of this step
+};
+
+template <int D, int P>
+struct Shape {
+    static constexpr int n = P + 1;
+    static constexpr int nf = P + 2;
+    static constexpr int V = D + 2;
+    static constexpr int NPT = D == 2 ? n * n : n * n * n;
+    static constexpr int NTP = NPT / n;    // points across one direction
+    static constexpr int NFP = NTP * nf;   // flux points per direction
+};
+
+// coordinates of a point index
+template <int n>
+__device__ __forceinline__ void pt_coords(int pt, int c[3]) {
+    c[0] = pt % n;
+    c[1] = (pt / n) % n;
+    c[2] = pt / (n * n);
+}
+template <int n>
+__device__ __forceinline__ int pt_index(const int c[3]) {
+    return c[0] + n * (c[1] + n * c[2]);
+}
+// flux-point index of direction d: extent nf along d, n along the others
+template <int n, int nf>
+__device__ __forceinline__ int fp_index(int d, const int c[3]) {
+    if (d == 0) return c[0] + nf * (c[1] + n * c[2]);
+    if (d == 1) return c[0] + n * (c[1] + nf * c[2]);
+    return c[0] + n * (c[1] + n * c[2]);
+}
+// transverse point tp of direction d -> coordinates (coordinate d untouched)
+template <int D, int n>
+__device__ __forceinline__ void tp_coords(int d, int tp, int c[3]) {
+    const int a = tp % n, b = tp / n;
+    if (d == 0) { c[1] = a; c[2] = D == 3 ? b : 0; }
+    else if (d == 1) { c[0] = a; c[2] = D == 3 ? b : 0; }
+    else { c[0] = a; c[1] = b; }
+}
+
+// Tile of TX x TY x TZ elements plus its face halo (no edges or corners).
+template <int D, int TX, int TY, int TZ>
+struct Tile {
+    static constexpr int NE = TX * TY * TZ;
+    static constexpr int HX = TY * TZ, HY = TX * TZ, HZ = TX * TY;
+    static constexpr int NS = NE + 2 * HX + 2 * HY + (D == 3 ? 2 * HZ : 0);
+    __device__ static int T(int d) { return d == 0 ? TX : (d == 1 ? TY : TZ); }
+    // slot of tile-local element coordinates (at most one outside the tile)
+    __device__ static int slot(int lx, int ly, int lz) {
+        if (lx < 0 || lx >= TX) return NE + (lx < 0 ? 0 : HX) + ly + TY * lz;
+        if (ly < 0 || ly >= TY) return NE + 2 * HX + (ly < 0 ? 0 : HY) + lx + TX * lz;
+        if (lz < 0 || lz >= TZ) return NE + 2 * HX + 2 * HY + (lz < 0 ? 0 : HZ) + lx + TX * ly;
+        return lx + TX * (ly + TY * lz);
+    }
+    // local coordinates of a slot
+    __device__ static void coords(int s, int l[3]) {
+        if (s < NE) {
+            l[0] = s % TX; l[1] = (s / TX) % TY; l[2] = s / (TX * TY);
+            return;
+        }
+        int r = s - NE;
+        if (r < 2 * HX) {
+            const int side = r / HX, q = r % HX;
+            l[0] = side ? TX : -1; l[1] = q % TY; l[2] = q / TY;
+            return;
+        }
+        r -= 2 * HX;
+        if (r < 2 * HY) {
+            const int side = r / HY, q = r % HY;
+            l[1] = side ? TY : -1; l[0] = q % TX; l[2] = q / TX;
+            return;
+        }
+        r -= 2 * HY;
+        const int side = r / HZ, q = r % HZ;
+        l[2] = side ? TZ : -1; l[0] = q % TX; l[1] = q / TX;
+    }
+};
+
+// global element index of tile-local coordinates, or -1 when the element
+// lies beyond a non-periodic domain edge
+template <int D>
+__device__ __forceinline__ long long elem_of(const DevGrid& G, const int o[3], const int l[3]) {
+    int g[3];
+    for (int d = 0; d < 3; d++) {
+        g[d] = o[d] + l[d];
+        if (d >= D) { g[d] = 0; continue; }
+        if (g[d] < 0 || g[d] >= G.N[d]) {
+            if (G.bc[d] != kPeriodic) return -1;
+            g[d] = g[d] < 0 ? g[d] + G.N[d] : g[d] - G.N[d];
+        }
+    }
+    return ((long long)g[2] * G.N[1] + g[1]) * G.N[0] + g[0];
+}
+
+// dt candidate of one W_cv point (src/hydro.cpp:222-254, inviscid)
+template <int D>
+__device__ __forceinline__ double point_dt(const DevGrid& G, const double* w, int n) {
+    const double cs = sound_speed(w[0], w[D + 1], G.gm);
+    double cmax = 0, dxmin = 1;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        cmax += (fabs(w[1 + d]) + cs);
+        dxmin = smin(dxmin, G.h[d]);
+    }
+    return G.cfl * dxmin / cmax / n;
+}
+
+// block-wide min of positive doubles, then one atomic per block (the order
+// of a min never changes its value)
+__device__ __forceinline__ void block_min_dt(double v, unsigned long long* out) {
+    __shared__ double red[kThreads / 32];
+    for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = l < (int)(blockDim.x >> 5) ? red[l] : 1.7976931348623157e308;
+        for (int o = 16; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (l == 0) atomicMin(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// One directional sweep of element-local arrays in shared memory
+// (src/transforms.cpp:120-147): out(c) = sum_l in(c with c_d = l) * M(c_d, l)
+template <int D, int P>
+__device__ __forceinline__ void sweep_smem(const double* in, double* out, const double* M, int d, int count) {
+    using S = Shape<D, P>;
+    constexpr int n = S::n;
+    for (int q = threadIdx.x; q < count; q += blockDim.x) {
+        const int pt = q % S::NPT, base = q - pt;
+        int c[3];
+        pt_coords<n>(pt, c);
+        const int id = c[d];
+        double u = 0;
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+            c[d] = l;
+            u += in[base + pt_index<n>(c)] * M[id * n + l];
+        }
+        out[q] = u;
+    }
+}
+
+// Sub-cell candidate of the FV update (src/transforms.cpp:483-543 with
+// update=0): U_new = U_old - (w_t dt) sum_d (F_{+} - F_{-}) / h_d for the
+// cell at point pt of element ge; F from FF_d of slice t.
+template <int D, int P>
+__device__ __forceinline__ void fv_candidate(const DevGrid& G, double* const* ff, int t, long long ge, int pt,
+                                             const double* uold, double wdt, double* unew) {
+    using S = Shape<D, P>;
+    constexpr int n = S::n, nf = S::nf, V = S::V;
+    int c[3];
+    pt_coords<n>(pt, c);
+    long long eg[3];
+    eg[0] = ge % G.N[0];
+    eg[1] = (ge / G.N[0]) % G.N[1];
+    eg[2] = ge / ((long long)G.N[0] * G.N[1]);
+    double hd[3];
+    int fl[3], fr[3];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        const long long I = eg[d] * n + c[d] + 2;
+        hd[d] = G.fvf[d][I + 1] - G.fvf[d][I];
+        int cc[3] = {c[0], c[1], c[2]};
+        fl[d] = fp_index<n, nf>(d, cc);
+        cc[d] = c[d] + 1;
+        fr[d] = fp_index<n, nf>(d, cc);
+    }
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        double F = 0;
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            const double* f = ff[d] + (((long long)t * G.E + ge) * V + v) * S::NFP;
+            F += (f[fr[d]] - f[fl[d]]) / hd[d];
+        }
+        if (G.grav) {
+            double s = 0;
+            if (v >= 1 && v <= D) s = uold[0] * G.g[v - 1];
+            else if (v == D + 1) {
+                s = uold[1] * G.g[0] + uold[2] * G.g[1];
+                if (D == 3) s = s + uold[3] * G.g[2];
+            }
+            if (v != 0) F -= s;
+        }
+        unew[v] = uold[v] - wdt * F;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Picard pass: interpolation to flux points, Euler fluxes, LLF at element
+// interfaces, flux divergence and the ADER predictor / corrector update,
+// fused so that only U_ader crosses HBM.
+// ---------------------------------------------------------------------------
+template <int D, int P, int TX, int TY, int TZ, int MODE>
+__global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, PicardArgs A) {
+    using S = Shape<D, P>;
+    using TL = Tile<D, TX, TY, TZ>;
+    constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
+    constexpr int NE = TL::NE, NS = TL::NS;
+    constexpr int PPT = (NE * NPT + kThreads - 1) / kThreads;
+    constexpr int NT = MODE == kFlux ? 1 : (P + 1);  // register slices kept per point
+
+    extern __shared__ double smem[];
+    double* Ss = smem;                       // [NS][V][NPT]
+    double* FX = Ss + NS * V * NPT;          // [D][NE][V][NFP]
+    double* TT = FX + D * NE * V * NFP;      // [NE][V][NFP] face-integral scratch (3D)
+    __shared__ long long sl_elem[NS];
+
+    const int tid = threadIdx.x;
+    int o[3];
+    {
+        int b = blockIdx.x;
+        const int tx = G.N[0] / TX, ty = G.N[1] / TY;
+        o[0] = (b % tx) * TX;
+        b /= tx;
+        o[1] = (b % ty) * TY;
+        b /= ty;
+        o[2] = D == 3 ? b * TZ : 0;
+    }
+    for (int s = tid; s < NS; s += kThreads) {
+        int l[3];
+        TL::coords(s, l);
+        sl_elem[s] = elem_of<D>(G, o, l);
+    }
+    const double dt = *A.dt;
+    const int nt = G.nt;
+    const long long E = G.E;
+
+    double dreg[PPT][V][NT];   // kPredict: dudt per slice; kCorrect: du in [..][..][0]
+#pragma unroll
+    for (int r = 0; r < PPT; r++)
+#pragma unroll
+        for (int v = 0; v < V; v++)
+#pragma unroll
+            for (int t = 0; t < NT; t++) dreg[r][v][t] = 0;
+
+    __syncthreads();
+    for (int t = 0; t < nt; t++) {
+        // ---- stage slice t of the tile and its face halo ----
+        if (t == 0 || A.in_slices > 1) {
+            const double* src = A.in_slices > 1 ? A.ua_in + (long long)t * E * V * NPT : A.ua_in;
+            for (int q = tid; q < NS * V * NPT; q += kThreads) {
+                const int s = q / (V * NPT), off = q - s * (V * NPT);
+                const long long ge = sl_elem[s];
+                if (ge >= 0) Ss[q] = src[ge * V * NPT + off];
+            }
+            __syncthreads();
+        }
+        // ---- phase A: flux-point fluxes of every direction ----
+        {
+            constexpr int NINT = NE * (nf - 2) * NTP;
+            int total = 0;
+            int base_int[3], base_face[3], nface[3];
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                base_int[d] = total;
+                total += NINT;
+                base_face[d] = total;
+                nface[d] = (TL::T(d) + 1) * (NE / TL::T(d)) * NTP;
+                total += nface[d];
+            }
+            for (int q = tid; q < total; q += kThreads) {
+                int d = 0;
+#pragma unroll
+                for (int dd = 1; dd < D; dd++)
+                    if (q >= base_int[dd]) d = dd;
+                const int n0 = 0;
+                (void)n0;
+                int c[3] = {0, 0, 0};
+                if (q < base_face[d]) {
+                    // interior flux point ll of element el
+                    const int r = q - base_int[d];
+                    const int el = r / ((nf - 2) * NTP);
+                    const int rr = r % ((nf - 2) * NTP);
+                    const int ll = 1 + rr / NTP, tp = rr % NTP;
+                    tp_coords<D, n>(d, tp, c);
+                    double u[V], w[V], f[V];
+                    const double* src = Ss + el * V * NPT;
+#pragma unroll
+                    for (int v = 0; v < V; v++) {
+                        double a = 0;
+#pragma unroll
+                        for (int l = 0; l < n; l++) {
+                            c[d] = l;
+                            a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[ll * n + l];
+                        }
+                        u[v] = a;
+                    }
+                    primitives<D>(u, w, G.gm);
+                    euler_flux<D>(u, w, f, d);
+                    c[d] = ll;
+                    const int fi = fp_index<n, nf>(d, c);
+                    double* dst = FX + (d * NE + el) * V * NFP;
+#pragma unroll
+                    for (int v = 0; v < V; v++) dst[v * NFP + fi] = f[v];
+                } else {
+                    // element interface fi_loc of direction d
+                    const int Td = TL::T(d);
+                    const int r = q - base_face[d];
+                    const int per = (NE / Td) * NTP;
+                    const int fidx = r / per;
+                    const int rr = r % per;
+                    const int qq = rr / NTP, tp = rr % NTP;
+                    tp_coords<D, n>(d, tp, c);
+                    int lL[3], lR[3];
+                    if (d == 0) { lL[1] = qq % TY; lL[2] = qq / TY; }
+                    else if (d == 1) { lL[0] = qq % TX; lL[2] = qq / TX; }
+                    else { lL[0] = qq % TX; lL[1] = qq / TX; }
+                    lL[d] = fidx - 1;
+                    lR[0] = lL[0]; lR[1] = lL[1]; lR[2] = lL[2];
+                    lR[d] = fidx;
+                    if (D == 2) { lL[2] = 0; lR[2] = 0; }
+                    const int gface = o[d] + fidx;
+                    const bool ghostL = gface == 0 && G.bc[d] != kPeriodic;
+                    const bool ghostR = gface == G.N[d] && G.bc[d] != kPeriodic;
+                    double uL[V], uR[V];
+                    if (!ghostL) {
+                        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * V * NPT;
+#pragma unroll
+                        for (int v = 0; v < V; v++) {
+                            double a = 0;
+#pragma unroll
+                            for (int l = 0; l < n; l++) {
+                                c[d] = l;
+                                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[(nf - 1) * n + l];
+                            }
+                            uL[v] = a;
+                        }
+                    }
+                    if (!ghostR) {
+                        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * V * NPT;
+#pragma unroll
+                        for (int v = 0; v < V; v++) {
+                            double a = 0;
+#pragma unroll
+                            for (int l = 0; l < n; l++) {
+                                c[d] = l;
+                                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[l];
+                            }
+                            uR[v] = a;
+                        }
+                    }
+                    // ghost interface state (src/boundary.cpp:48-113)
+                    if (ghostL) {
+#pragma unroll
+                        for (int v = 0; v < V; v++) uL[v] = uR[v];
+                        if (G.bc[d] == kReflective) uL[1 + d] = -uL[1 + d];
+                    }
+                    if (ghostR) {
+#pragma unroll
+                        for (int v = 0; v < V; v++) uR[v] = uL[v];
+                        if (G.bc[d] == kReflective) uR[1 + d] = -uR[1 + d];
+                    }
+                    double F[V];
+                    riemann_llf<D>(F, uL, uR, d, G.gm);
+                    if (fidx >= 1) {
+                        c[d] = nf - 1;
+                        const int fi = fp_index<n, nf>(d, c);
+                        double* dst = FX + (d * NE + TL::slot(lL[0], lL[1], lL[2])) * V * NFP;
+#pragma unroll
+                        for (int v = 0; v < V; v++) dst[v * NFP + fi] = F[v];
+                    }
+                    if (fidx < Td) {
+                        c[d] = 0;
+                        const int fi = fp_index<n, nf>(d, c);
+                        double* dst = FX + (d * NE + TL::slot(lR[0], lR[1], lR[2])) * V * NFP;
+#pragma unroll
+                        for (int v = 0; v < V; v++) dst[v * NFP + fi] = F[v];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (MODE != kFlux) {
+            // ---- phase B: flux divergence at the solution points ----
+#pragma unroll
+            for (int r = 0; r < PPT; r++) {
+                const int q = tid + r * kThreads;
+                if (q < NE * NPT) {
+                    const int el = q / NPT, pt = q % NPT;
+                    int c[3];
+                    pt_coords<n>(pt, c);
+                    int fpi[3][kMaxNfd];
+#pragma unroll
+                    for (int d = 0; d < D; d++) {
+                        int cc[3] = {c[0], c[1], c[2]};
+#pragma unroll
+                        for (int ll = 0; ll < nf; ll++) {
+                            cc[d] = ll;
+                            fpi[d][ll] = fp_index<n, nf>(d, cc);
+                        }
+                    }
+#pragma unroll
+                    for (int v = 0; v < V; v++) {
+                        double dudt = 0;
+#pragma unroll
+                        for (int ll = 0; ll < nf; ll++) {
+#pragma unroll
+                            for (int d = 0; d < D; d++) {
+                                const double Fv = FX[((d * NE + el) * V + v) * NFP + fpi[d][ll]];
+                                dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], G.h[d], G.rh[d], G.pow2[d] != 0);
+                            }
+                        }
+                        if (MODE == kPredict) {
+#pragma unroll
+                            for (int tt = 0; tt < NT; tt++)
+                                if (tt == t) dreg[r][v][tt] = dudt;
+                        } else {
+                            if (G.grav && v != 0) {
+                                const double* uv = Ss + el * V * NPT;
+                                double s;
+                                if (v <= D) s = uv[pt] * G.g[v - 1];
+                                else {
+                                    s = uv[NPT + pt] * G.g[0] + uv[2 * NPT + pt] * G.g[1];
+                                    if (D == 3) s = s + uv[3 * NPT + pt] * G.g[2];
+                                }
+                                dudt -= s;
+                            }
+                            dreg[r][v][0] += dudt * M.wt[t] * dt;
+                        }
+                    }
+                }
+            }
+        } else {
+            // ---- FV face fluxes of slice t (src/transforms.cpp:378-481) ----
+            const double* Mc = M.sp_to_cv;
+#pragma unroll
+            for (int d = 0; d < D; d++) {
+                double* out = A.ff[d];
+                const double* Fd = FX + d * NE * V * NFP;
+                if (D == 2) {
+                    for (int q = tid; q < NE * V * NFP; q += kThreads) {
+                        const int el = q / (V * NFP);
+                        const int rem = q % (V * NFP);
+                        const int v = rem / NFP, fi = rem % NFP;
+                        // fi = (face ll along d, transverse cell c)
+                        int ll, cc;
+                        if (d == 0) { ll = fi % nf; cc = fi / nf; }
+                        else { cc = fi % n; ll = fi / n; }
+                        double f = 0;
+#pragma unroll
+                        for (int m = 0; m < n; m++) {
+                            const int src = d == 0 ? (ll + nf * m) : (m + n * ll);
+                            f += Fd[(el * V + v) * NFP + src] * Mc[cc * n + m];
+                        }
+                        out[(((long long)t * E + sl_elem[el]) * V + v) * NFP + fi] = f;
+                    }
+                } else {
+                    // two transverse sweeps: dim1 = next(d), dim2 = next(dim1)
+                    const int d1 = d == 0 ? 1 : (d == 1 ? 2 : 0);
+                    const int d2 = d1 == 0 ? 1 : (d1 == 1 ? 2 : 0);
+                    for (int q = tid; q < NE * V * NFP; q += kThreads) {
+                        const int base = q - q % NFP;
+                        const int fi = q % NFP;
+                        int c[3];
+                        // decode face index of direction d
+                        if (d == 0) { c[0] = fi % nf; c[1] = (fi / nf) % n; c[2] = fi / (nf * n); }
+                        else if (d == 1) { c[0] = fi % n; c[1] = (fi / n) % nf; c[2] = fi / (n * nf); }
+                        else { c[0] = fi % n; c[1] = (fi / n) % n; c[2] = fi / (n * n); }
+                        const int id = c[d1];
+                        double u = 0;
+#pragma unroll
+                        for (int m = 0; m < n; m++) {
+                            c[d1] = m;
+                            u += Fd[base + fp_index<n, nf>(d, c)] * Mc[id * n + m];
+                        }
+                        TT[q] = u;
+                    }
+                    __syncthreads();
+                    for (int q = tid; q < NE * V * NFP; q += kThreads) {
+                        const int base = q - q % NFP;
+                        const int fi = q % NFP;
+                        const int el = q / (V * NFP), v = (q / NFP) % V;
+                        int c[3];
+                        if (d == 0) { c[0] = fi % nf; c[1] = (fi / nf) % n; c[2] = fi / (nf * n); }
+                        else if (d == 1) { c[0] = fi % n; c[1] = (fi / n) % nf; c[2] = fi / (n * nf); }
+                        else { c[0] = fi % n; c[1] = (fi / n) % n; c[2] = fi / (n * n); }
+                        const int id = c[d2];
+                        double f = 0;
+#pragma unroll
+                        for (int m = 0; m < n; m++) {
+                            c[d2] = m;
+                            f += TT[base + fp_index<n, nf>(d, c)] * Mc[id * n + m];
+                        }
+                        out[(((long long)t * E + sl_elem[el]) * V + v) * NFP + fi] = f;
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    if (MODE == kPredict) {
+        // ---- ADER predictor (src/transforms.cpp:309-323) ----
+#pragma unroll
+        for (int r = 0; r < PPT; r++) {
+            const int q = tid + r * kThreads;
+            if (q < NE * NPT) {
+                const int el = q / NPT, pt = q % NPT;
+                const long long ge = sl_elem[el];
+                double nw[D + 1][NT];  // updated rho and momenta (gravity of later slots)
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    const double u_old = A.u[(ge * V + v) * NPT + pt];
+                    double dudt[NT];
+#pragma unroll
+                    for (int tt = 0; tt < NT; tt++) {
+                        dudt[tt] = dreg[r][v][tt];
+                        if (G.grav && v != 0 && tt < nt) {
+                            double s;
+                            if (v <= D) s = nw[0][tt] * G.g[v - 1];
+                            else {
+                                s = nw[1][tt] * G.g[0] + nw[2][tt] * G.g[1];
+                                if (D == 3) s = s + nw[3][tt] * G.g[2];
+                            }
+                            dudt[tt] -= s;
+                        }
+                    }
+#pragma unroll
+                    for (int tt = 0; tt < NT; tt++) {
+                        if (tt >= nt) break;
+                        double du = 0;
+#pragma unroll
+                        for (int ll = 0; ll < NT; ll++)
+                            if (ll < nt) du += dudt[ll] * M.invader[tt * nt + ll] * M.wt[ll] * dt;
+                        const double val = u_old - du;
+                        if (v <= D) nw[v][tt] = val;
+                        A.ua_out[(((long long)tt * E + ge) * V + v) * NPT + pt] = val;
+                    }
+                }
+            }
+        }
+    } else if (MODE == kCorrect) {
+        // ---- corrector / RK stage (src/transforms.cpp:327-374, 252-261) ----
+        double* Wsp = Ss;                  // reuse staging memory: [NE][V][NPT]
+        double* Tmp = Ss + NE * V * NPT;
+#pragma unroll
+        for (int r = 0; r < PPT; r++) {
+            const int q = tid + r * kThreads;
+            if (q < NE * NPT) {
+                const int el = q / NPT, pt = q % NPT;
+                const long long ge = sl_elem[el];
+                double un[V];
+#pragma unroll
+                for (int v = 0; v < V; v++) {
+                    const long long gi = (ge * V + v) * NPT + pt;
+                    double val = A.u[gi] - dreg[r][v][0];
+                    if (A.rk_a > 0) val = A.rk_a * A.u0[gi] + (1.0 - A.rk_a) * val;
+                    un[v] = val;
+                    A.u_out[gi] = val;
+                }
+                if (A.final_stage) {
+                    double w[V];
+                    primitives<D>(un, w, G.gm);
+#pragma unroll
+                    for (int v = 0; v < V; v++) Wsp[(el * V + v) * NPT + pt] = w[v];
+                }
+            }
+        }
+        if (A.final_stage) {
+            __syncthreads();
+            // W_cv = sp_to_cv(W_sp): x, y(, z) sweeps (src/transforms.cpp:99-117)
+            double* bufs[2] = {Tmp, Wsp};
+            const double* src = Wsp;
+            for (int d = 0; d < D; d++) {
+                double* dst = bufs[d % 2];
+                sweep_smem<D, P>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+                __syncthreads();
+                src = dst;
+            }
+            double dtl = 1.7976931348623157e308;
+#pragma unroll
+            for (int r = 0; r < PPT; r++) {
+                const int q = tid + r * kThreads;
+                if (q < NE * NPT) {
+                    const int el = q / NPT, pt = q % NPT;
+                    const long long ge = sl_elem[el];
+                    double w[V];
+#pragma unroll
+                    for (int v = 0; v < V; v++) w[v] = src[(el * V + v) * NPT + pt];
+                    if (A.wcv)
+#pragma unroll
+                        for (int v = 0; v < V; v++) A.wcv[(ge * V + v) * NPT + pt] = w[v];
+                    dtl = smin(dtl, point_dt<D>(G, w, n));
+                }
+            }
+            block_min_dt(dtl, A.dtmin);
+        }
+    } else {
+        // ---- U_cv = sp_to_cv(U) and the slice-0 FV candidate ----
+        double* Ut = Ss;
+        double* Tmp = Ss + NE * V * NPT;
+        for (int q = tid; q < NE * V * NPT; q += kThreads) {
+            const int el = q / (V * NPT), off = q % (V * NPT);
+            Ut[q] = A.u[sl_elem[el] * V * NPT + off];
+        }
+        __syncthreads();
+        double* bufs[2] = {Tmp, Ut};
+        const double* src = Ut;
+        for (int d = 0; d < D; d++) {
+            double* dst = bufs[d % 2];
+            sweep_smem<D, P>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+            __syncthreads();
+            src = dst;
+        }
+        for (int q = tid; q < NE * V * NPT; q += kThreads) {
+            const int el = q / (V * NPT), off = q % (V * NPT);
+            A.ucv[sl_elem[el] * V * NPT + off] = src[q];
+        }
+        for (int q = tid; q < NE * NPT; q += kThreads) {
+            const int el = q / NPT, pt = q % NPT;
+            const long long ge = sl_elem[el];
+            double uo[V], un[V], w[V];
+#pragma unroll
+            for (int v = 0; v < V; v++) uo[v] = src[(el * V + v) * NPT + pt];
+            fv_candidate<D, P>(G, A.ff, 0, ge, pt, uo, M.wt[0] * dt, un);
+            primitives<D>(uo, w, G.gm);
+            A.rp_old[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
+            primitives<D>(un, w, G.gm);
+            A.rp_new[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
+        }
+    }
+}
+
+template <int D, int P, int TX, int TY, int TZ>
+constexpr size_t picard_smem_bytes() {
+    using S = Shape<D, P>;
+    using TL = Tile<D, TX, TY, TZ>;
+    size_t a = (size_t)TL::NS * S::V * S::NPT;
+    size_t b = (size_t)D * TL::NE * S::V * S::NFP;
+    size_t c = (size_t)TL::NE * S::V * S::NFP;
+    size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
+    size_t total = a + b + c;
+    if (need_epi > total) total = need_epi;
+    return total * sizeof(double);
+}
+
+}  // namespace spdk
