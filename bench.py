@@ -1,0 +1,408 @@
+"""Benchmark of the spd_K B200 hydro step (one JSON line on rank 0).
+
+Workload: the 2D point blast with the a-posteriori limiter -- 256x256
+elements, p=3 (16 solution points per element, 1,048,576 DOF), gamma=1.4,
+unit box with outflow (gradfree) boundaries, rho=1, v=0, P=1e-5 outside and
+P=(gamma-1)E/(pi r^2) with E=1 inside r=0.01, ADER time stepping, LLF at SD
+faces, NAD (relative tolerance 1e-5, Moore neighbourhood) + SED + PAD
+detection with theta blending of MUSCL-Hancock/HLLC fallback fluxes. The
+initial condition is generated, not read: data = "synthetic".
+
+A step is one full ADER step (p+1 Picard passes + p+1 fallback slices +
+dt reduction). The metric is DOF-updates/s = active solution points x steps
+/ seconds (the reference's "zone-cycles/s", src/hydro_ader.hpp:263-271).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N>1 runs N independent replicas (one per GPU, weak scaling); the headline
+time is the max over ranks of CUDA-event time on each solver stream.
+"""
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "blast2d-256x256-p3-ader-nad-muscl"
+P0_BLAST = 0.4 / (math.pi * 0.01 ** 2)  # (gamma-1) E / (pi r^2), E = 1, r = 0.01
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload_overrides(N=256, p=3):
+    return [
+        "job/system=hydro", "job/fallback=true", f"mesh/p={p}", f"mesh/nx1={N}", f"mesh/nx2={N}",
+        "mesh/nx3=1", "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "time/cfl=0.8",
+        "time/integrator=ader", "hydro/gamma=1.4", "problem/problem=spherical_blast",
+        "problem/d0=1.0", f"problem/p0={P0_BLAST!r}", "problem/p1=1e-5", "problem/radius=0.01",
+        "fallback/tolerance=1e-5", "output/dt=-1",
+    ]
+
+
+def workload_config(N=256, p=3):
+    from spd_k_b200.api import apply_overrides, config_from_params
+    return config_from_params(apply_overrides({}, workload_overrides(N, p)))
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                      "-i", str(self.index), "-lms", "100"],
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel kind (FP64 parity form)
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(info, fallback):
+    """Compulsory HBM bytes of one launch of each kernel kind; S = one state
+    array (E x V x NPT doubles)."""
+    E, V, npt, nt, D, p = info.n_elements, info.nvar, info.n_points, info.n_time_slices, info.ndim, info.p
+    n, nf = p + 1, p + 2
+    S = E * V * npt * 8
+    cells = E * npt
+    ff_slice = D * E * V * (npt // n) * nf * 8          # FV face fluxes of one slice
+    b = {}
+    # predictor: first pass reads U once and writes nt slices; later passes
+    # read nt slices + U and write nt slices; averaged over the p passes
+    first = S + nt * S
+    later = nt * S + S + nt * S
+    b["predict"] = (first + (nt - 2) * later) / max(nt - 1, 1)
+    b["correct"] = nt * S + S + S + S                    # U_ader, U (r+w), W_cv
+    b["flux"] = nt * S + S + nt * ff_slice + S + 2 * cells * 16   # U_ader, U, FF, U_cv, candidates
+    b["detect"] = 2 * cells * 16 + cells                  # (rho,p) candidates -> flags
+    b["theta"] = cells + cells
+    b["update"] = S + ff_slice + cells + S + (2 * cells * 16 if True else 0)
+    return b
+
+
+KINDS = ["predict", "correct", "flux", "detect", "theta", "update", "other"]
+
+
+def traffic_from_profiles(kind):
+    """dram bytes per launch of a kernel kind from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            j = json.load(f)
+        v = j.get(WORKLOAD, {}).get(kind)
+        return float(v) if v is not None else None
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU build (oracle/_ref) or the oracle port
+# ---------------------------------------------------------------------------
+def reference_cpu_run(steps, N=256, p=3, dt0=None):
+    """Run the reference binary for `steps` full-size steps; returns
+    (DOF-updates/s, ms/step, steps, threads, kind, sample)."""
+    threads = os.cpu_count() or 1
+    ref = os.path.join(ROOT, "oracle", "_ref", "spd_K_ref")
+    if dt0 is None:
+        dt0 = reference_dt0(N, p)
+    tlim = (steps - 0.5) * dt0
+    if os.path.exists(ref):
+        with tempfile.TemporaryDirectory() as tmp:
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads), SPD_OUTPUT_DIR=tmp)
+            cmd = [ref] + workload_overrides(N, p) + [f"time/tlim={tlim!r}"]
+            r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=1800)
+            m = re.search(r"evolution: (\d+) steps, ([\d.eE+-]+) s \(([\d.eE+-]+) ms/step\), ([\d.eE+-]+) zone-cycles/s",
+                          r.stdout)
+            if r.returncode == 0 and m:
+                return (float(m.group(4)), float(m.group(3)), int(m.group(1)), threads, "reference",
+                        f"reference CPU build (sources compiled unmodified with a Kokkos-subset OpenMP shim), "
+                        f"{N}x{N} p={p}, {m.group(1)} full-size steps, OMP_NUM_THREADS={threads}")
+    # oracle port (single thread) on the same workload
+    from oracle import oracle as O
+    c = O.config_from_params(O.apply_overrides({}, workload_overrides(N, p)))
+    o = O.Oracle(c)
+    dt = o.compute_dt()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step(dt)
+        dt = o.compute_dt()
+    el = time.perf_counter() - t0
+    dof = N * N * (p + 1) ** 2
+    return (dof * steps / el, el / steps * 1e3, steps, 1, "port",
+            f"C restatement of the reference path (oracle port), {N}x{N} p={p}, {steps} steps, 1 thread")
+
+
+def reference_dt0(N=256, p=3):
+    from oracle import oracle as O
+    c = O.config_from_params(O.apply_overrides({}, workload_overrides(N, p)))
+    # the initial dt depends only on the initial state; the oracle computes it exactly
+    return O.Oracle(c).compute_dt()
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        return rank, world, local, dist
+    return rank, world, local, None
+
+
+def max_over_ranks(dist, value, device):
+    """max of a per-rank value (device: "cuda:<local>" under NCCL, "cpu" under gloo)"""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_throughput(world, dof_per_rank, steps, ms_max):
+    """whole-job DOF-updates/s of `world` replicas, timed by the slowest rank"""
+    return world * dof_per_rank * steps / (ms_max * 1e-3)
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def run_reference_arm(args):
+    rank, world, local, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+                                int(os.environ.get("LOCAL_RANK", "0")), None)
+    if rank != 0:
+        return 0
+    steps = max(1, min(args.steps, args.ref_steps))
+    val, ms, ran, threads, kind, sample = reference_cpu_run(steps)
+    line = {
+        "impl": "reference", "metric": "DOF-updates/s", "value": val, "unit": "DOF-updates/s",
+        "n_gpus": args.gpus, "steps": ran, "warmup": 0, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "elements": [256, 256], "p": 3, "dof": 256 * 256 * 16,
+                   "integrator": "ader", "fallback": "NAD+SED+PAD, theta-blended MUSCL-Hancock/HLLC"},
+        "cpu_baseline": {"value": val, "unit": "DOF-updates/s", "cores": threads, "kind": kind, "sample": sample},
+        "e2e": {"value": val, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--profile-steps", type=int, default=20)
+    ap.add_argument("--ref-steps", type=int, default=3, help="full-size steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--N", type=int, default=256)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    import ctypes
+    import numpy as np
+    import spd_k_b200 as S
+    from spd_k_b200.api import _lib
+
+    c = workload_config(args.N)
+    solver = S.HydroSolver(c, device=local)
+    L = S.load_library()
+    info = solver.info
+    dof = info.n_dof
+
+    # ---- headline: K graph-replayed steps, inputs resident in HBM ----
+    import torch
+    torch.cuda.set_device(local)
+    sp = ctypes.c_void_p()
+    L.spdk_hydro_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    rc = L.spdk_hydro_get_stream(solver.h, ctypes.byref(sp))
+    assert rc == 0
+    stream = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
+    solver.steps(args.warmup)
+    solver.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier(dist)
+    torch.cuda.synchronize()
+    solver.sync()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    solver.steps(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    solver.sync()
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms_local = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, ms_local, f"cuda:{local}")
+    value = aggregate_throughput(world, dof, args.steps, ms)
+
+    # ---- per-kernel CUDA-event pass (same stream, no graph) ----
+    L.spdk_hydro_profile.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_longlong)]
+    kms = (ctypes.c_double * 7)()
+    kl = (ctypes.c_longlong * 7)()
+    rc = L.spdk_hydro_profile(solver.h, args.profile_steps, kms, kl)
+    assert rc == 0, _lib.spdk_last_error()
+    per_kind = {KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i]),
+                           "avg_us": (1e3 * kms[i] / kl[i]) if kl[i] else None} for i in range(7)}
+    alg = algorithmic_bytes(info, c["fallback"])
+    dom = max((k for k in KINDS if k in alg and per_kind[k]["launches"]), key=lambda k: per_kind[k]["ms"])
+    hbm, peak_kind = peaks()
+    achieved = alg[dom] / (per_kind[dom]["avg_us"] * 1e-6) / 1e9
+    traffic = traffic_from_profiles(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes": alg[dom]}
+    kernel_table = {k: dict(v, algorithmic_gbs=(alg[k] / (v["avg_us"] * 1e-6) / 1e9
+                                                 if k in alg and v["avg_us"] else None))
+                    for k, v in per_kind.items() if v["launches"]}
+
+    # ---- e2e through the C ABI with host buffers (reference driver loop) ----
+    solver2 = S.HydroSolver(c, device=local)
+    u_host = torch.empty(info.n_elements * info.nvar * info.n_points, dtype=torch.float64,
+                         pin_memory=True).numpy()
+    solver2.read(S.FIELD_U_SP, out=u_host)
+    w_host = torch.empty_like(torch.from_numpy(u_host)).pin_memory().numpy()
+    rc = L.spdk_hydro_get_stream(solver2.h, ctypes.byref(sp))
+    stream2 = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
+    e2e_steps = max(1, min(args.steps, 200))
+    barrier(dist)
+    solver2.sync()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream2)
+    solver2.write_u(u_host)                 # H2D of the job's input state (pinned)
+    for _ in range(e2e_steps):
+        solver2.step()                      # spdk_hydro_step
+        solver2.dt()                        # blocking D2H of the step's dt, as time_evolution does
+    solver2.read(S.FIELD_W_CV, out=w_host)  # D2H of the result
+    f1.record(stream2)
+    f1.synchronize()
+    e2e_ms = max_over_ranks(dist, f0.elapsed_time(f1), f"cuda:{local}")
+    state_bytes = u_host.nbytes
+    e2e = {"value": world * dof * e2e_steps / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
+           "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": 8 + state_bytes / e2e_steps,
+           "steps": e2e_steps, "path": "spdk_hydro_write + spdk_hydro_step/get_dt per step + spdk_hydro_read"}
+    solver2.close()
+
+    # ---- CPU baseline (rank 0, N=1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            val, ms_ref, ran, threads, kind, sample = reference_cpu_run(args.ref_steps)
+            cpu = {"value": val, "unit": "DOF-updates/s", "cores": threads, "kind": kind, "sample": sample}
+        except Exception as ex:  # reported, not fatal
+            cpu = {"value": None, "unit": "DOF-updates/s", "cores": 0, "kind": "unavailable", "sample": str(ex)[:200]}
+
+    barrier(dist)
+    if rank == 0:
+        state_gb = info.device_bytes / 1e9
+        line = {
+            "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "elements": [args.N, args.N], "p": 3, "dof_per_gpu": dof,
+                       "integrator": "ader", "riemann": "LLF at SD faces, HLLC at fallback faces",
+                       "fallback": "NAD(1e-5, Moore)+SED+PAD, theta-blended MUSCL-Hancock",
+                       "precision": "fp64, reference operation order (plain form)",
+                       "parallelism": f"replicas{world}",
+                       "l2": f"no flush: device working set {state_gb:.2f} GB > 126 MB L2",
+                       "state": "steps continue from the initial blast after the warm-up"},
+            "gpu_launches": info.launches_per_step * args.steps,
+            "roofline": roofline,
+            "kernels": kernel_table,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -121,10 +121,40 @@ int spdk_hydro_steps(spdk_hydro* h, int n);
  * output times exactly. Returns the number of steps and the final t. */
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t);
 int spdk_hydro_sync(spdk_hydro* h);
+/* the CUDA stream (cudaStream_t) every solver launch is ordered on */
+int spdk_hydro_get_stream(spdk_hydro* h, void** stream);
+/* kernel kinds timed by spdk_hydro_profile */
+enum {
+    SPDK_KERNEL_PREDICT = 0,  /* Picard predictor pass */
+    SPDK_KERNEL_CORRECT = 1,  /* corrector / RK stage + W_cv + dt */
+    SPDK_KERNEL_FLUX = 2,     /* last Picard pass writing FV face fluxes */
+    SPDK_KERNEL_DETECT = 3,   /* NAD/SED/PAD */
+    SPDK_KERNEL_THETA = 4,    /* theta blending */
+    SPDK_KERNEL_UPDATE = 5,   /* fallback fluxes + FV update (+ W_cv, dt) */
+    SPDK_KERNEL_OTHER = 6,    /* dt hand-over */
+    SPDK_KERNEL_KINDS = 7
+};
+/* run n steps without graph replay, bracketing every launch with CUDA events
+ * on the solver stream; adds the device time (ms) and launch count of each
+ * kernel kind to ms[kind] and launches[kind] (arrays of SPDK_KERNEL_KINDS) */
+int spdk_hydro_profile(spdk_hydro* h, int n, double* ms, long long* launches);
 /* copy a field to / from host memory (count = number of doubles); writing
  * SPDK_FIELD_U_SP recomputes W_cv and dt */
 int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count);
 int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count);
+
+/* Host-only set-up (no GPU needed).
+ * spdk_build_matrices: the transform matrices of degree p, as the reference
+ * builds them in Hydro_ader::Hydro_ader (src/hydro_ader.hpp:129-141, from
+ * src/polynomials.cpp): sp_to_fp [(p+2)(p+1)], dfp_to_sp [(p+1)(p+2)],
+ * sp_to_cv and cv_to_sp [(p+1)^2], invader [(p+1)^2, ADER only] and the time
+ * weights wt [p+1]. Any output pointer may be NULL. */
+int spdk_build_matrices(int p, int ader, double* sp_to_fp, double* dfp_to_sp, double* sp_to_cv,
+                        double* cv_to_sp, double* invader, double* wt);
+/* spdk_initial_wcv: the initial primitive sub-cell averages of a
+ * configuration (src/initial_conditions.cpp:179-228) in the solver layout
+ * [element][var][point]; count = elements * (ndim+2) * points. */
+int spdk_initial_wcv(const spdk_hydro_config* cfg, double* out, size_t count);
 
 #ifdef __cplusplus
 }

@@ -13,8 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspdk_cuda.so")
-SOURCES = ["spdk_hydro.cu", "spdk_setup.cpp"]
-HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_setup.h"]
+SOURCES = ["spdk_hydro.cu", "spdk_select_2d_low.cu", "spdk_select_2d_high.cu", "spdk_select_3d.cu",
+           "spdk_setup.cpp", "spdk_host_api.cpp"]
+HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_kernelset.cuh", "spdk_setup.h"]
 
 
 def nvcc_path():

@@ -9,8 +9,7 @@
 #include <vector>
 
 #include "spdk.h"
-#include "spdk_fallback.cuh"
-#include "spdk_kernels.cuh"
+#include "spdk_kernelset.cuh"
 #include "spdk_setup.h"
 
 namespace spdk {
@@ -28,157 +27,6 @@ int fail(int code, const std::string& msg) {
         if (e_ != cudaSuccess)                                                           \
             return fail(SPDK_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
-
-// ---------------------------------------------------------------------------
-// element-local set-up kernels
-// ---------------------------------------------------------------------------
-// U_sp = conservatives(cv_to_sp(W_cv)) and dt(W_cv): the constructor tail
-// (src/hydro_ader.hpp:205-208)
-template <int D, int P>
-__global__ void __launch_bounds__(kThreads) init_state_kernel(DevGrid G, DevMats M, const double* __restrict__ wcv,
-                                                             double* __restrict__ u,
-                                                             unsigned long long* dtmin) {
-    using S = Shape<D, P>;
-    constexpr int V = S::V, NPT = S::NPT;
-    __shared__ double b0[V * NPT], b1[V * NPT];
-    const long long ge = blockIdx.x;
-    for (int q = threadIdx.x; q < V * NPT; q += blockDim.x) b0[q] = wcv[ge * V * NPT + q];
-    __syncthreads();
-    double dtl = 1.7976931348623157e308;
-    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V];
-        for (int v = 0; v < V; v++) w[v] = b0[v * NPT + q];
-        dtl = smin(dtl, point_dt<D>(G, w, S::n));
-    }
-    double* bufs[2] = {b1, b0};
-    const double* src = b0;
-    for (int d = 0; d < D; d++) {
-        double* dst = bufs[d % 2];
-        sweep_smem<D, P>(src, dst, M.cv_to_sp, d, V * NPT);
-        __syncthreads();
-        src = dst;
-    }
-    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V], uu[V];
-        for (int v = 0; v < V; v++) w[v] = src[v * NPT + q];
-        conservatives<D>(w, uu, G.gm);
-        for (int v = 0; v < V; v++) u[ge * V * NPT + v * NPT + q] = uu[v];
-    }
-    block_min_dt(dtl, dtmin);
-}
-
-// W_cv = sp_to_cv(primitives(U_sp)) and dt, for a state written by the host
-template <int D, int P>
-__global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMats M, const double* __restrict__ u,
-                                                         double* __restrict__ wcv, unsigned long long* dtmin) {
-    using S = Shape<D, P>;
-    constexpr int V = S::V, NPT = S::NPT;
-    __shared__ double b0[V * NPT], b1[V * NPT];
-    const long long ge = blockIdx.x;
-    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double uu[V], w[V];
-        for (int v = 0; v < V; v++) uu[v] = u[ge * V * NPT + v * NPT + q];
-        primitives<D>(uu, w, G.gm);
-        for (int v = 0; v < V; v++) b0[v * NPT + q] = w[v];
-    }
-    __syncthreads();
-    double* bufs[2] = {b1, b0};
-    const double* src = b0;
-    for (int d = 0; d < D; d++) {
-        double* dst = bufs[d % 2];
-        sweep_smem<D, P>(src, dst, M.sp_to_cv, d, V * NPT);
-        __syncthreads();
-        src = dst;
-    }
-    double dtl = 1.7976931348623157e308;
-    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V];
-        for (int v = 0; v < V; v++) {
-            w[v] = src[v * NPT + q];
-            wcv[ge * V * NPT + v * NPT + q] = w[v];
-        }
-        dtl = smin(dtl, point_dt<D>(G, w, S::n));
-    }
-    block_min_dt(dtl, dtmin);
-}
-
-// next dt <- reduced minimum; re-arm the reduction
-__global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin) {
-    *dt = __longlong_as_double((long long)*dtmin);
-    *dtmin = 0x7FEFFFFFFFFFFFFFULL;
-}
-
-// ---------------------------------------------------------------------------
-// kernel table of one (D, P, tile) instantiation
-// ---------------------------------------------------------------------------
-struct KernelSet {
-    void (*predict)(DevGrid, DevMats, PicardArgs) = nullptr;
-    void (*correct)(DevGrid, DevMats, PicardArgs) = nullptr;
-    void (*flux)(DevGrid, DevMats, PicardArgs) = nullptr;
-    void (*detect)(DevGrid, const double2*, const double2*, uint8_t*, int*) = nullptr;
-    void (*theta)(DevGrid, const uint8_t*, uint8_t*) = nullptr;
-    void (*update)(DevGrid, DevMats, FallbackArgs) = nullptr;
-    void (*init)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
-    void (*derive)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
-    size_t picard_smem = 0, update_smem = 0;
-    int tile[3] = {1, 1, 1};
-};
-
-template <int D, int P, int TX, int TY, int TZ>
-KernelSet make_set() {
-    KernelSet k;
-    k.predict = picard_kernel<D, P, TX, TY, TZ, kPredict>;
-    k.correct = picard_kernel<D, P, TX, TY, TZ, kCorrect>;
-    k.flux = picard_kernel<D, P, TX, TY, TZ, kFlux>;
-    k.detect = fv_detect_kernel<D, P>;
-    k.theta = fv_theta_kernel<D, P, TX, TY, TZ>;
-    k.update = fv_update_kernel<D, P, TX, TY, TZ>;
-    k.init = init_state_kernel<D, P>;
-    k.derive = derive_kernel<D, P>;
-    k.picard_smem = picard_smem_bytes<D, P, TX, TY, TZ>();
-    k.update_smem = UpdateSmem<D, P, TX, TY, TZ>::bytes;
-    k.tile[0] = TX;
-    k.tile[1] = TY;
-    k.tile[2] = TZ;
-    return k;
-}
-
-// Tile choice: the largest instantiated tile that divides the element counts.
-template <int P>
-bool pick2(int Nx, int Ny, KernelSet* k) {
-    if (P <= 4 && Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
-    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<2, P, 2, 2, 1>(); return true; }
-    *k = make_set<2, P, 1, 1, 1>();
-    return true;
-}
-template <int P>
-bool pick3(int, int, int, KernelSet* k) {
-    *k = make_set<3, P, 1, 1, 1>();
-    return true;
-}
-
-bool select_kernels(int D, int p, const int N[3], KernelSet* k) {
-    if (D == 2) {
-        switch (p) {
-        case 1: return pick2<1>(N[0], N[1], k);
-        case 2: return pick2<2>(N[0], N[1], k);
-        case 3: return pick2<3>(N[0], N[1], k);
-        case 4: return pick2<4>(N[0], N[1], k);
-        case 5: return pick2<5>(N[0], N[1], k);
-        case 6: return pick2<6>(N[0], N[1], k);
-        case 7: return pick2<7>(N[0], N[1], k);
-        }
-    } else if (D == 3) {
-        switch (p) {
-        case 1: return pick3<1>(N[0], N[1], N[2], k);
-        case 2: return pick3<2>(N[0], N[1], N[2], k);
-        case 3: return pick3<3>(N[0], N[1], N[2], k);
-        case 4: return pick3<4>(N[0], N[1], N[2], k);
-        case 5: return pick3<5>(N[0], N[1], N[2], k);
-        }
-    }
-    return false;
-}
 
 }  // namespace spdk
 
@@ -205,6 +53,11 @@ struct spdk_hydro {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     int launches = 0;
+    // per-launch event timing (spdk_hydro_profile)
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_kind;
+    size_t ev_used = 0;
 };
 
 namespace {
@@ -215,6 +68,25 @@ int dalloc(spdk_hydro* h, void** p, size_t bytes) {
         return fail(SPDK_E_NOMEM, "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
     h->bytes += bytes;
     return 0;
+}
+
+// open / close an event bracket around one launch when profiling
+void prof_begin(spdk_hydro* h) {
+    if (!h->profiling) return;
+    if (h->ev_used + 2 > h->ev.size()) {
+        for (int q = 0; q < 64; q++) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            h->ev.push_back(e);
+        }
+    }
+    cudaEventRecord(h->ev[h->ev_used], h->stream);
+}
+void prof_end(spdk_hydro* h, int kind) {
+    if (!h->profiling) return;
+    cudaEventRecord(h->ev[h->ev_used + 1], h->stream);
+    h->ev_kind.push_back(kind);
+    h->ev_used += 2;
 }
 
 unsigned grid_blocks(const spdk_hydro* h) {
@@ -244,7 +116,9 @@ int enqueue_step(spdk_hydro* h) {
             A.ua_in = in;
             A.in_slices = in_slices;
             A.ua_out = h->ua[it % 2];
+            prof_begin(h);
             k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            prof_end(h, SPDK_KERNEL_PREDICT);
             launches++;
             in = h->ua[it % 2];
             in_slices = h->nt;
@@ -258,18 +132,26 @@ int enqueue_step(spdk_hydro* h) {
             A.final_stage = final_stage;
             A.wcv = h->wcv;
             A.dtmin = h->dtmin;
+            prof_begin(h);
             k.correct<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            prof_end(h, SPDK_KERNEL_CORRECT);
             launches++;
         } else {
             for (int d = 0; d < 3; d++) A.ff[d] = h->ff[d];
             A.ucv = h->ucv[0];
             A.rp_old = h->rpo;
             A.rp_new = h->rpn;
+            prof_begin(h);
             k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            prof_end(h, SPDK_KERNEL_FLUX);
             launches++;
             for (int t = 0; t < h->nt; t++) {
+                prof_begin(h);
                 k.detect<<<cells_blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
+                prof_end(h, SPDK_KERNEL_DETECT);
+                prof_begin(h);
                 k.theta<<<blocks, kThreads, 0, h->stream>>>(h->G, h->trouble, h->theta);
+                prof_end(h, SPDK_KERNEL_THETA);
                 FallbackArgs F{};
                 F.ucv_in = h->ucv[t % 2];
                 F.ucv_out = h->ucv[(t + 1) % 2];
@@ -291,12 +173,16 @@ int enqueue_step(spdk_hydro* h) {
                 F.wcv = h->wcv;
                 F.dtmin = h->dtmin;
                 F.dt = h->dt;
+                prof_begin(h);
                 k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, h->dm, F);
+                prof_end(h, SPDK_KERNEL_UPDATE);
                 launches += 3;
             }
         }
     }
+    prof_begin(h);
     advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+    prof_end(h, SPDK_KERNEL_OTHER);
     launches++;
     h->launches = launches;
     SPDK_CUDA(cudaGetLastError());
@@ -305,6 +191,7 @@ int enqueue_step(spdk_hydro* h) {
 
 void release(spdk_hydro* h) {
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
                     h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
                     h->rpo, h->rpn, h->trouble, h->theta, h->dtmin};
@@ -530,6 +417,35 @@ int spdk_hydro_steps(spdk_hydro* h, int nsteps) {
     }
     for (int s = 0; s < nsteps; s++) SPDK_CUDA(cudaGraphLaunch(h->graph, h->stream));
     return 0;
+}
+
+int spdk_hydro_get_stream(spdk_hydro* h, void** stream) {
+    if (!h || !stream) return fail(SPDK_E_ARG, "null argument");
+    *stream = (void*)h->stream;
+    return 0;
+}
+
+int spdk_hydro_profile(spdk_hydro* h, int nsteps, double* ms, long long* launches) {
+    if (!h || !ms || !launches || nsteps < 0) return fail(SPDK_E_ARG, "bad argument");
+    h->profiling = true;
+    h->ev_used = 0;
+    h->ev_kind.clear();
+    int rc = 0;
+    for (int s = 0; s < nsteps && !rc; s++) {
+        rc = enqueue_step(h);
+        if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = fail(SPDK_E_CUDA, "profile sync");
+        for (size_t q = 0; q < h->ev_kind.size() && !rc; q++) {
+            float t = 0;
+            if (cudaEventElapsedTime(&t, h->ev[2 * q], h->ev[2 * q + 1]) != cudaSuccess)
+                rc = fail(SPDK_E_CUDA, "event timing");
+            ms[h->ev_kind[q]] += t;
+            launches[h->ev_kind[q]] += 1;
+        }
+        h->ev_used = 0;
+        h->ev_kind.clear();
+    }
+    h->profiling = false;
+    return rc;
 }
 
 int spdk_hydro_sync(spdk_hydro* h) {

@@ -1,0 +1,151 @@
+// Kernel table of one (ndim, p, tile) instantiation and the element-local
+// set-up kernels. Instantiated in spdk_select_*.cu so the (ndim, p) variants
+// compile in parallel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "spdk_fallback.cuh"
+#include "spdk_kernels.cuh"
+
+namespace spdk {
+
+// ---------------------------------------------------------------------------
+// element-local set-up kernels
+// ---------------------------------------------------------------------------
+// U_sp = conservatives(cv_to_sp(W_cv)) and dt(W_cv): the constructor tail
+// (src/hydro_ader.hpp:205-208)
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads) init_state_kernel(DevGrid G, DevMats M, const double* __restrict__ wcv,
+                                                             double* __restrict__ u,
+                                                             unsigned long long* dtmin) {
+    using S = Shape<D, P>;
+    constexpr int V = S::V, NPT = S::NPT;
+    __shared__ double b0[V * NPT], b1[V * NPT];
+    const long long ge = blockIdx.x;
+    for (int q = threadIdx.x; q < V * NPT; q += blockDim.x) b0[q] = wcv[ge * V * NPT + q];
+    __syncthreads();
+    double dtl = 1.7976931348623157e308;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V];
+        for (int v = 0; v < V; v++) w[v] = b0[v * NPT + q];
+        dtl = smin(dtl, point_dt<D>(G, w, S::n));
+    }
+    double* bufs[2] = {b1, b0};
+    const double* src = b0;
+    for (int d = 0; d < D; d++) {
+        double* dst = bufs[d % 2];
+        sweep_smem<D, P>(src, dst, M.cv_to_sp, d, V * NPT);
+        __syncthreads();
+        src = dst;
+    }
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V], uu[V];
+        for (int v = 0; v < V; v++) w[v] = src[v * NPT + q];
+        conservatives<D>(w, uu, G.gm);
+        for (int v = 0; v < V; v++) u[ge * V * NPT + v * NPT + q] = uu[v];
+    }
+    block_min_dt(dtl, dtmin);
+}
+
+// W_cv = sp_to_cv(primitives(U_sp)) and dt, for a state written by the host
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMats M, const double* __restrict__ u,
+                                                         double* __restrict__ wcv, unsigned long long* dtmin) {
+    using S = Shape<D, P>;
+    constexpr int V = S::V, NPT = S::NPT;
+    __shared__ double b0[V * NPT], b1[V * NPT];
+    const long long ge = blockIdx.x;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double uu[V], w[V];
+        for (int v = 0; v < V; v++) uu[v] = u[ge * V * NPT + v * NPT + q];
+        primitives<D>(uu, w, G.gm);
+        for (int v = 0; v < V; v++) b0[v * NPT + q] = w[v];
+    }
+    __syncthreads();
+    double* bufs[2] = {b1, b0};
+    const double* src = b0;
+    for (int d = 0; d < D; d++) {
+        double* dst = bufs[d % 2];
+        sweep_smem<D, P>(src, dst, M.sp_to_cv, d, V * NPT);
+        __syncthreads();
+        src = dst;
+    }
+    double dtl = 1.7976931348623157e308;
+    for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
+        double w[V];
+        for (int v = 0; v < V; v++) {
+            w[v] = src[v * NPT + q];
+            wcv[ge * V * NPT + v * NPT + q] = w[v];
+        }
+        dtl = smin(dtl, point_dt<D>(G, w, S::n));
+    }
+    block_min_dt(dtl, dtmin);
+}
+
+// next dt <- reduced minimum; re-arm the reduction
+static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin) {
+    *dt = __longlong_as_double((long long)*dtmin);
+    *dtmin = 0x7FEFFFFFFFFFFFFFULL;
+}
+
+// ---------------------------------------------------------------------------
+// kernel table of one (D, P, tile) instantiation
+// ---------------------------------------------------------------------------
+struct KernelSet {
+    void (*predict)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*correct)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*flux)(DevGrid, DevMats, PicardArgs) = nullptr;
+    void (*detect)(DevGrid, const double2*, const double2*, uint8_t*, int*) = nullptr;
+    void (*theta)(DevGrid, const uint8_t*, uint8_t*) = nullptr;
+    void (*update)(DevGrid, DevMats, FallbackArgs) = nullptr;
+    void (*init)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
+    void (*derive)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
+    size_t picard_smem = 0, update_smem = 0;
+    int tile[3] = {1, 1, 1};
+};
+
+template <int D, int P, int TX, int TY, int TZ>
+KernelSet make_set() {
+    KernelSet k;
+    k.predict = picard_kernel<D, P, TX, TY, TZ, kPredict>;
+    k.correct = picard_kernel<D, P, TX, TY, TZ, kCorrect>;
+    k.flux = picard_kernel<D, P, TX, TY, TZ, kFlux>;
+    k.detect = fv_detect_kernel<D, P>;
+    k.theta = fv_theta_kernel<D, P, TX, TY, TZ>;
+    k.update = fv_update_kernel<D, P, TX, TY, TZ>;
+    k.init = init_state_kernel<D, P>;
+    k.derive = derive_kernel<D, P>;
+    k.picard_smem = picard_smem_bytes<D, P, TX, TY, TZ>();
+    k.update_smem = UpdateSmem<D, P, TX, TY, TZ>::bytes;
+    k.tile[0] = TX;
+    k.tile[1] = TY;
+    k.tile[2] = TZ;
+    return k;
+}
+
+// Tile choice: the largest instantiated tile that divides the element counts.
+template <int P>
+bool pick2(int Nx, int Ny, KernelSet* k) {
+    if (P <= 4 && Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
+    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<2, P, 2, 2, 1>(); return true; }
+    *k = make_set<2, P, 1, 1, 1>();
+    return true;
+}
+template <int P>
+bool pick3(int, int, int, KernelSet* k) {
+    *k = make_set<3, P, 1, 1, 1>();
+    return true;
+}
+
+// per-translation-unit selectors (spdk_select_*.cu)
+bool select_2d_low(int p, const int N[3], KernelSet* k);   // p = 1..3
+bool select_2d_high(int p, const int N[3], KernelSet* k);  // p = 4..7
+bool select_3d(int p, const int N[3], KernelSet* k);       // p = 1..5
+
+inline bool select_kernels(int D, int p, const int N[3], KernelSet* k) {
+    if (D == 2) return p <= 3 ? select_2d_low(p, N, k) : select_2d_high(p, N, k);
+    if (D == 3) return select_3d(p, N, k);
+    return false;
+}
+
+}  // namespace spdk

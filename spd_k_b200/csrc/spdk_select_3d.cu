@@ -1,0 +1,17 @@
+// Kernel instantiations of one group of (ndim, p) variants.
+#include "spdk_kernelset.cuh"
+
+namespace spdk {
+
+bool select_3d(int p, const int N[3], KernelSet* k) {
+    switch (p) {
+    case 1: return pick3<1>(N[0], N[1], N[2], k);
+    case 2: return pick3<2>(N[0], N[1], N[2], k);
+    case 3: return pick3<3>(N[0], N[1], N[2], k);
+    case 4: return pick3<4>(N[0], N[1], N[2], k);
+    case 5: return pick3<5>(N[0], N[1], N[2], k);
+    }
+    return false;
+}
+
+}  // namespace spdk

@@ -1,0 +1,130 @@
+"""Generate the parity fixtures from the reference's own CPU build.
+
+Runs oracle/_ref/spd_K_ref (the reference sources compiled unmodified; see
+oracle/Makefile) on small configurations given as block/name=value
+overrides of the reference defaults, and stores, per case:
+  <case>.npz     the active region of W_cv (slots rho, vx, vy, vz, p) at the
+                 last output, shape (5, Nz, Ny, Nx, nz, ny, nx), and the
+                 output time and step count
+  manifest.json  the overrides, the output index and the SHA-256 of the
+                 reference's raw output file
+It also records the SHA-256 of the reference's committed goldens
+(tests/goldens/ in the reference tree). Needs the reference tree; run once:
+    python tests/golden/make_fixtures.py
+"""
+import hashlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "spd_K_ref")
+REF_TREE = "/root/reference"
+
+BLAST = ["problem/problem=spherical_blast", "hydro/gamma=1.6666666666667"]
+CASES = {
+    # the reference's own regression set (tests/run_tests.py:44-143), 2D, small
+    "sine2d_ader": ["job/fallback=false", "mesh/nx3=1", "time/tlim=0.1", "output/dt=0.1"],
+    "sine2d_rk3": ["job/fallback=false", "mesh/nx3=1", "time/integrator=rk3", "time/tlim=0.1", "output/dt=0.1"],
+    "sine2d_fallback": ["job/fallback=true", "mesh/nx3=1", "time/tlim=0.1", "output/dt=0.1"],
+    "blast2d_fallback": ["job/fallback=true", "mesh/nx3=1", *BLAST, "time/tlim=0.02", "output/dt=0.02"],
+    "blast2d_rk3_fallback": ["job/fallback=true", "mesh/nx3=1", *BLAST, "time/integrator=rk3",
+                             "time/tlim=0.02", "output/dt=0.02"],
+    "implosion2d_reflective": ["job/fallback=true", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1",
+                               "mesh/x1len=0.3", "mesh/x2len=0.3", "mesh/x1_bc=reflective",
+                               "mesh/x2_bc=reflective", "problem/problem=implosion", "time/tlim=0.05",
+                               "output/dt=0.05"],
+    # the point-blast geometry of the benchmark workload at 16x16
+    "blast2d_gradfree_p3": ["job/fallback=true", "mesh/nx1=16", "mesh/nx2=16", "mesh/nx3=1",
+                            "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "problem/problem=spherical_blast",
+                            "problem/p0=1273.2395447351628", "problem/p1=1e-5", "problem/radius=0.05",
+                            "time/tlim=0.002", "output/dt=0.002"],
+    "kh2d_p2": ["job/fallback=true", "mesh/p=2", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1",
+                "problem/problem=kelvin_helmholtz", "time/tlim=0.05", "output/dt=0.05"],
+    "rti2d_gravity": ["job/fallback=true", "mesh/nx1=4", "mesh/nx2=8", "mesh/nx3=1", "mesh/x1len=0.5",
+                      "mesh/x2len=1.0", "mesh/x2_bc=reflective", "problem/problem=rti", "hydro/g2=-0.1",
+                      "time/tlim=0.05", "output/dt=0.05"],
+    # 1-D profile problems run as quasi-2D strips
+    "sod2d_p4": ["job/fallback=true", "mesh/p=4", "mesh/nx1=16", "mesh/nx2=2", "mesh/nx3=1",
+                 "mesh/x1_bc=gradfree", "problem/problem=sod_shock_tube", "time/tlim=0.05", "output/dt=0.05"],
+}
+# full-size run of the plain-method CPU-runnable configuration (2D sine,
+# 32x32, p=3, ADER, LLF, to t=1): only rho and p are stored, with the
+# SHA-256 of the active rho, vx, vy, p slots
+FULL_CASES = {
+    "config1_sine2d_32": ["job/fallback=false", "mesh/nx1=32", "mesh/nx2=32", "mesh/nx3=1",
+                          "time/tlim=1.0", "output/dt=1.0"],
+}
+GOLDENS = {
+    "hydro_sd/W_cv_N8p3_1_0.dat": "reference golden: 3D sine wave, N=8, p=3, ADER, t=0.1",
+    "induction_fv/B2_cv_N8p3_2_0.dat": "reference golden: 3D induction loop with fallback, t=0.2",
+}
+
+
+def sha256(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        h.update(f.read())
+    return h.hexdigest()
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    manifest = {"cases": {}, "goldens": {}}
+    for name, ov in CASES.items():
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out, OMP_NUM_THREADS="8")
+            r = subprocess.run([REF_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            files = sorted(f for f in os.listdir(out) if f.startswith("W_cv_"))
+            last = max(files, key=lambda f: int(f.split("_")[-2]))
+            raw = np.fromfile(os.path.join(out, last))
+            # shape from the coordinate files: active faces per direction
+            def n_el(axis):
+                fs = [f for f in os.listdir(out) if f.startswith(axis + "_N")]
+                return int(fs[0].split("_N")[1].split("p")[0]), int(fs[0].split("p")[1].split("_")[0])
+            (Nx, p), (Ny, _), (Nz, _) = n_el("X"), n_el("Y"), n_el("Z")
+            n = p + 1
+            act = lambda N: N > 1
+            shape = (1, 6, Nz + 2 if act(Nz) else 1, Ny + 2, Nx + 2, n if act(Nz) else 1, n, n)
+            w = raw.reshape(shape)[0, :5]
+            w = w[:, 1:-1] if act(Nz) else w
+            w = w[:, :, 1:-1, 1:-1]
+            steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), W_cv=np.ascontiguousarray(w))
+            manifest["cases"][name] = {"overrides": ov, "output": last, "steps": steps,
+                                       "sha256": sha256(os.path.join(out, last)),
+                                       "shape": list(w.shape)}
+            print(name, last, w.shape, steps, flush=True)
+    for name, ov in FULL_CASES.items():
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out, OMP_NUM_THREADS="8")
+            r = subprocess.run([REF_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            last = sorted(f for f in os.listdir(out) if f.startswith("W_cv_"))[-1]
+            raw = np.fromfile(os.path.join(out, last))
+            N = 32
+            w = raw.reshape(1, 6, 1, N + 2, N + 2, 1, 4, 4)[0, :5, :, 1:-1, 1:-1]
+            act4 = np.ascontiguousarray(w[[0, 1, 2, 4]])
+            steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), rho=np.ascontiguousarray(w[0]),
+                                p=np.ascontiguousarray(w[4]))
+            manifest["full_cases"] = manifest.get("full_cases", {})
+            manifest["full_cases"][name] = {"overrides": ov, "output": last, "steps": steps,
+                                            "sha256_active_rho_vx_vy_p": hashlib.sha256(act4.tobytes()).hexdigest()}
+            print(name, last, steps, flush=True)
+    for rel, what in GOLDENS.items():
+        path = os.path.join(REF_TREE, "tests", "goldens", rel)
+        if os.path.exists(path):
+            manifest["goldens"][rel] = {"sha256": sha256(path), "what": what}
+    with open(os.path.join(HERE, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
