@@ -269,6 +269,8 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=3, help="full-size steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--N", type=int, default=256)
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch the timed steps one by one instead of replaying the step graph")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -295,7 +297,11 @@ def main():
     rc = L.spdk_hydro_get_stream(solver.h, ctypes.byref(sp))
     assert rc == 0
     stream = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
-    solver.steps(args.warmup)
+    if args.no_graph:
+        for _ in range(args.warmup):
+            solver.step()
+    else:
+        solver.steps(args.warmup)
     solver.sync()
     clocks = ClockSampler(local)
     clocks.start()
@@ -306,7 +312,11 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    solver.steps(args.steps)
+    if args.no_graph:
+        for _ in range(args.steps):
+            solver.step()
+    else:
+        solver.steps(args.steps)
     e1.record(stream)
     e1.synchronize()
     solver.sync()

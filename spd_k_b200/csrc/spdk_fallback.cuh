@@ -70,112 +70,138 @@ __device__ __forceinline__ double rp_var(const double2 v, int k) { return k == 0
 
 // ---------------------------------------------------------------------------
 // Trouble detection of every active sub-cell (src/trouble_detection.cpp:35-290
-// with limit mask rho|p, src/hydro_ader.hpp:522-524)
+// with limit mask rho|p, src/hydro_ader.hpp:522-524).
+//
+// The SED relaxation can only clear a flag NAD raised (relax_NAD keeps a
+// flag iff alpha < 1), so the division-heavy smooth-extrema indicator is
+// evaluated only at cells NAD flagged; the result is identical to computing
+// it everywhere. W_old (rho, p) of the tile + 1 halo is staged in shared
+// memory for the NAD box.
 // ---------------------------------------------------------------------------
 template <int D, int P>
+__device__ __forceinline__ double sed_component(const DevGrid& G, const double2* __restrict__ rpn, const int a[3],
+                                                int d, int k) {
+    constexpr int n = P + 1;
+    const int nd = G.N[d] * n;
+    const double* C = G.fvc[d];
+    const double* Fc = G.fvf[d];
+    double al[3];
+    bool fl[3];
+#pragma unroll
+    for (int s = -1; s <= 1; s++) {
+        const int ad = a[d] + s;
+        if (ad < 0 || ad >= nd) { al[s + 1] = 0.0; continue; }  // never computed outside the active cells
+        int b[3] = {a[0], a[1], a[2]};
+        double Wv[5];
+#pragma unroll
+        for (int off = -2; off <= 2; off++) {
+            b[d] = ad + off;
+            Wv[off + 2] = rp_var(rpn[cell_image<D, P>(G, b, fl)], k);
+        }
+        const int l = ad + 2;
+        const double h = (C[l + 1] - C[l - 1]);
+        const double hp = (C[l + 2] - C[l]);
+        const double hm = (C[l] - C[l - 2]);
+        const double u = Wv[2];
+        const double du = (Wv[3] - Wv[1]) / h;
+        const double dup = (Wv[4] - u) / hp;
+        const double dum = (u - Wv[0]) / hm;
+        const double d2u = (dup - dum) / (C[l + 1] - C[l - 1]);
+        const double dv = 0.5 * d2u * (Fc[l + 1] - Fc[l]);
+        al[s + 1] = sed_alpha(dv, dum, du, dup);
+    }
+    return smin(smin(al[0], al[1]), al[2]);
+}
+
+template <int D, int P, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
                                                             uint8_t* __restrict__ T, int* any_trouble) {
     constexpr int n = P + 1;
     constexpr int NPT = Shape<D, P>::NPT;
-    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= G.E * NPT) return;
-    const long long ge = q / NPT;
-    const int pt = (int)(q - ge * NPT);
-    int c[3];
-    pt_coords<n>(pt, c);
-    int a[3] = {0, 0, 0};
+    constexpr int Bx = TX * n, By = TY * n, Bz = D == 3 ? TZ * n : 1;
+    constexpr int E1x = Bx + 2, E1y = By + 2, E1z = D == 3 ? Bz + 2 : 1;
+    __shared__ double2 Ro[E1x * E1y * E1z];
+    const int dz = D == 3 ? 1 : 0;
+    int o[3];
     {
-        long long r = ge;
-#pragma unroll
-        for (int d = 0; d < D; d++) {
-            const long long ed = r % G.N[d];
-            r /= G.N[d];
-            a[d] = (int)(ed * n) + c[d];
-        }
+        int b = blockIdx.x;
+        const int tx = G.N[0] / TX, ty = G.N[1] / TY;
+        o[0] = (b % tx) * Bx;
+        b /= tx;
+        o[1] = (b % ty) * By;
+        b /= ty;
+        o[2] = D == 3 ? b * Bz : 0;
     }
-    const double2 here_new = rpn[q];
-    double flag[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const double un = rp_var(here_new, k);
-        double mx = rp_var(rpo[q], k), mn = mx;
+    for (int q = threadIdx.x; q < E1x * E1y * E1z; q += blockDim.x) {
+        int a[3] = {o[0] - 1 + q % E1x, o[1] - 1 + (q / E1x) % E1y, o[2] - dz + q / (E1x * E1y)};
         bool fl[3];
-        if (G.nad_moore) {
-            const int dz = D == 3 ? 1 : 0;
-            for (int ok = -dz; ok <= dz; ok++)
-                for (int oj = -1; oj <= 1; oj++)
-                    for (int oi = -1; oi <= 1; oi++) {
-                        int b[3] = {a[0] + oi, a[1] + oj, a[2] + ok};
-                        const double u = rp_var(rpo[cell_image<D, P>(G, b, fl)], k);
-                        mx = smax(mx, u);
-                        mn = smin(mn, u);
-                    }
-        } else {
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                int bl[3] = {a[0], a[1], a[2]}, br[3] = {a[0], a[1], a[2]};
-                bl[d] -= 1;
-                br[d] += 1;
-                const double uL = rp_var(rpo[cell_image<D, P>(G, bl, fl)], k);
-                const double uR = rp_var(rpo[cell_image<D, P>(G, br, fl)], k);
-                mx = smax(smax(uL, mx), uR);
-                mn = smin(smin(uL, mn), uR);
-            }
-        }
-        if (G.nad_delta) {
-            const double eps = G.nad_tol * (mx - mn);
-            mn -= eps;
-            mx += eps;
-        } else {
-            mn -= fabs(mn) * G.nad_tol;
-            mx += fabs(mx) * G.nad_tol;
-        }
-        double f = (un > mx || un < mn) ? 1.0 : 0.0;
-        if (G.use_sed) {
-            double alpha = 1;
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                const int nd = G.N[d] * n;
-                const double* C = G.fvc[d];
-                const double* Fc = G.fvf[d];
-                double al[3];
-#pragma unroll
-                for (int s = -1; s <= 1; s++) {
-                    const int ad = a[d] + s;
-                    if (ad < 0 || ad >= nd) { al[s + 1] = 0.0; continue; }  // never computed there
-                    int b[3] = {a[0], a[1], a[2]};
-                    auto W = [&](int off) {
-                        b[d] = ad + off;
-                        return rp_var(rpn[cell_image<D, P>(G, b, fl)], k);
-                    };
-                    const int l = ad + 2;
-                    const double h = (C[l + 1] - C[l - 1]);
-                    const double hp = (C[l + 2] - C[l]);
-                    const double hm = (C[l] - C[l - 2]);
-                    const double u = W(0);
-                    const double du = (W(1) - W(-1)) / h;
-                    const double dup = (W(2) - u) / hp;
-                    const double dum = (u - W(-2)) / hm;
-                    const double d2u = (dup - dum) / (C[l + 1] - C[l - 1]);
-                    const double dv = 0.5 * d2u * (Fc[l + 1] - Fc[l]);
-                    al[s + 1] = sed_alpha(dv, dum, du, dup);
-                }
-                const double m3 = smin(smin(al[0], al[1]), al[2]);
-                alpha = d == 0 ? m3 : smin(alpha, m3);
-            }
-            f = alpha < 1 ? f : 0;
-        }
-        flag[k] = f;
+        Ro[q] = rpo[cell_image<D, P>(G, a, fl)];
     }
-    double tr = 0;
-    tr = smax(tr, flag[0]);
-    tr = smax(tr, flag[1]);
-    const double rho = here_new.x, p = here_new.y;
-    if (rho < kRhoMin || rho > kRhoMax) tr = 1;
-    if (p < kPMin || p > kPMax) tr = 1;
-    T[q] = tr > 0 ? 1 : 0;
-    if (any_trouble && tr > 0) atomicAdd(any_trouble, 1);
+    __syncthreads();
+    for (int q = threadIdx.x; q < Bx * By * Bz; q += blockDim.x) {
+        const int x = q % Bx, y = (q / Bx) % By, z = q / (Bx * By);
+        int a[3] = {o[0] + x, o[1] + y, o[2] + z};
+        const long long cid = cell_id<D, P>(G, a);
+        const double2 here_new = rpn[cid];
+        const int sc = (x + 1) + E1x * ((y + 1) + E1y * (z + dz));
+        double flag[2];
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const double un = rp_var(here_new, k);
+            double mx = rp_var(Ro[sc], k), mn = mx;
+            if (G.nad_moore) {
+                for (int ok = -dz; ok <= dz; ok++)
+#pragma unroll
+                    for (int oj = -1; oj <= 1; oj++)
+#pragma unroll
+                        for (int oi = -1; oi <= 1; oi++) {
+                            const double u = rp_var(Ro[sc + oi + E1x * (oj + E1y * ok)], k);
+                            mx = smax(mx, u);
+                            mn = smin(mn, u);
+                        }
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; d++) {
+                    const int st = d == 0 ? 1 : (d == 1 ? E1x : E1x * E1y);
+                    const double uL = rp_var(Ro[sc - st], k);
+                    const double uR = rp_var(Ro[sc + st], k);
+                    mx = smax(smax(uL, mx), uR);
+                    mn = smin(smin(uL, mn), uR);
+                }
+            }
+            if (G.nad_delta) {
+                const double eps = G.nad_tol * (mx - mn);
+                mn -= eps;
+                mx += eps;
+            } else {
+                mn -= fabs(mn) * G.nad_tol;
+                mx += fabs(mx) * G.nad_tol;
+            }
+            flag[k] = (un > mx || un < mn) ? 1.0 : 0.0;
+        }
+        if (G.use_sed) {
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                if (flag[k] == 0.0) continue;  // relaxation cannot raise a flag
+                double alpha = 1;
+#pragma unroll
+                for (int d = 0; d < D; d++) {
+                    const double m3 = sed_component<D, P>(G, rpn, a, d, k);
+                    alpha = d == 0 ? m3 : smin(alpha, m3);
+                }
+                flag[k] = alpha < 1 ? flag[k] : 0;
+            }
+        }
+        double tr = 0;
+        tr = smax(tr, flag[0]);
+        tr = smax(tr, flag[1]);
+        const double rho = here_new.x, p = here_new.y;
+        if (rho < kRhoMin || rho > kRhoMax) tr = 1;
+        if (p < kPMin || p > kPMax) tr = 1;
+        T[cid] = tr > 0 ? 1 : 0;
+        if (any_trouble && tr > 0) atomicAdd(any_trouble, 1);
+    }
 }
 
 // cell box of an element tile with a halo of g cells per active side

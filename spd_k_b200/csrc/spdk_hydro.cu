@@ -99,7 +99,6 @@ unsigned grid_blocks(const spdk_hydro* h) {
 int enqueue_step(spdk_hydro* h) {
     const KernelSet& k = h->ks;
     const unsigned blocks = grid_blocks(h);
-    const unsigned cells_blocks = (unsigned)((h->E * h->NPT + kThreads - 1) / kThreads);
     int launches = 0;
     if (h->nstages > 1)
         SPDK_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)h->E * h->V * h->NPT * sizeof(double),
@@ -147,7 +146,7 @@ int enqueue_step(spdk_hydro* h) {
             launches++;
             for (int t = 0; t < h->nt; t++) {
                 prof_begin(h);
-                k.detect<<<cells_blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
+                k.detect<<<blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
                 prof_end(h, SPDK_KERNEL_DETECT);
                 prof_begin(h);
                 k.theta<<<blocks, kThreads, 0, h->stream>>>(h->G, h->trouble, h->theta);
@@ -274,6 +273,9 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         G.rh[d] = G.pow2[d] ? std::ldexp(1.0, 1 - ex) : 0.0;
         G.g[d] = c.g[d];
     }
+    G.uniform_pow2 = 1;
+    for (int d = 0; d < D; d++)
+        if (!G.pow2[d] || G.h[d] != G.h[0]) G.uniform_pow2 = 0;
     G.gm = c.gamma;
     G.cfl = c.cfl;
     G.grav = (c.g[0] != 0.0 || c.g[1] != 0.0 || c.g[2] != 0.0) ? 1 : 0;

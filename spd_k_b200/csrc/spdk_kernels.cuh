@@ -40,6 +40,7 @@ struct DevGrid {
     int bc[3];
     double h[3], rh[3];
     int pow2[3];
+    int uniform_pow2;  // all active h equal and a power of two
     double gm, cfl;
     double g[3];
     int grav;
@@ -80,6 +81,16 @@ struct Shape {
     static constexpr int NPT = D == 2 ? n * n : n * n * n;
     static constexpr int NTP = NPT / n;    // points across one direction
     static constexpr int NFP = NTP * nf;   // flux points per direction
+};
+
+// padded shared-memory strides of the Picard pass (bank spreading)
+template <int D, int P>
+struct PicardPad {
+    static constexpr int V = D + 2;
+    static constexpr int NPT = D == 2 ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1);
+    static constexpr int NFP = NPT / (P + 1) * (P + 2);
+    static constexpr int SS = V * NPT + ((V * NPT) % 32 == 0 ? 2 : 0);
+    static constexpr int FXS = NFP + ((NFP * V) % 16 == 0 ? 1 : 0);
 };
 
 // coordinates of a point index
@@ -272,10 +283,14 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
     constexpr int PPT = (NE * NPT + kThreads - 1) / kThreads;
     constexpr int NT = MODE == kFlux ? 1 : (P + 1);  // register slices kept per point
 
+    // padded strides: an element block of the staged state (SS) and a
+    // variable row of the flux-point arrays (FXS) start on different banks
+    constexpr int SS = PicardPad<D, P>::SS;
+    constexpr int FXS = PicardPad<D, P>::FXS;
     extern __shared__ double smem[];
-    double* Ss = smem;                       // [NS][V][NPT]
-    double* FX = Ss + NS * V * NPT;          // [D][NE][V][NFP]
-    double* TT = FX + D * NE * V * NFP;      // [NE][V][NFP] face-integral scratch (3D)
+    double* Ss = smem;                       // [NS][SS >= V*NPT]
+    double* FX = Ss + NS * SS;               // [D][NE][V][FXS >= NFP]
+    double* TT = FX + D * NE * V * FXS;      // [NE][V][NFP] face-integral scratch (3D)
     __shared__ long long sl_elem[NS];
 
     const int tid = threadIdx.x;
@@ -314,40 +329,30 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
             for (int q = tid; q < NS * V * NPT; q += kThreads) {
                 const int s = q / (V * NPT), off = q - s * (V * NPT);
                 const long long ge = sl_elem[s];
-                if (ge >= 0) Ss[q] = src[ge * V * NPT + off];
+                if (ge >= 0) Ss[s * SS + off] = src[ge * V * NPT + off];
             }
             __syncthreads();
         }
         // ---- phase A: flux-point fluxes of every direction ----
-        {
+        // one loop per direction (compile-time d after unrolling): interior
+        // flux points first, then the element interfaces of the tile
+#pragma unroll
+        for (int d = 0; d < D; d++) {
             constexpr int NINT = NE * (nf - 2) * NTP;
-            int total = 0;
-            int base_int[3], base_face[3], nface[3];
-#pragma unroll
-            for (int d = 0; d < D; d++) {
-                base_int[d] = total;
-                total += NINT;
-                base_face[d] = total;
-                nface[d] = (TL::T(d) + 1) * (NE / TL::T(d)) * NTP;
-                total += nface[d];
-            }
+            const int Td = TL::T(d);
+            const int per = (NE / Td) * NTP;
+            const int total = NINT + (Td + 1) * per;
+            double* FXd = FX + d * NE * V * FXS;
             for (int q = tid; q < total; q += kThreads) {
-                int d = 0;
-#pragma unroll
-                for (int dd = 1; dd < D; dd++)
-                    if (q >= base_int[dd]) d = dd;
-                const int n0 = 0;
-                (void)n0;
                 int c[3] = {0, 0, 0};
-                if (q < base_face[d]) {
+                if (q < NINT) {
                     // interior flux point ll of element el
-                    const int r = q - base_int[d];
-                    const int el = r / ((nf - 2) * NTP);
-                    const int rr = r % ((nf - 2) * NTP);
+                    const int el = q / ((nf - 2) * NTP);
+                    const int rr = q % ((nf - 2) * NTP);
                     const int ll = 1 + rr / NTP, tp = rr % NTP;
                     tp_coords<D, n>(d, tp, c);
                     double u[V], w[V], f[V];
-                    const double* src = Ss + el * V * NPT;
+                    const double* src = Ss + el * SS;
 #pragma unroll
                     for (int v = 0; v < V; v++) {
                         double a = 0;
@@ -362,32 +367,29 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                     euler_flux<D>(u, w, f, d);
                     c[d] = ll;
                     const int fi = fp_index<n, nf>(d, c);
-                    double* dst = FX + (d * NE + el) * V * NFP;
+                    double* dst = FXd + el * V * FXS;
 #pragma unroll
-                    for (int v = 0; v < V; v++) dst[v * NFP + fi] = f[v];
+                    for (int v = 0; v < V; v++) dst[v * FXS + fi] = f[v];
                 } else {
-                    // element interface fi_loc of direction d
-                    const int Td = TL::T(d);
-                    const int r = q - base_face[d];
-                    const int per = (NE / Td) * NTP;
+                    // element interface fidx of direction d
+                    const int r = q - NINT;
                     const int fidx = r / per;
                     const int rr = r % per;
                     const int qq = rr / NTP, tp = rr % NTP;
                     tp_coords<D, n>(d, tp, c);
-                    int lL[3], lR[3];
+                    int lL[3] = {0, 0, 0};
                     if (d == 0) { lL[1] = qq % TY; lL[2] = qq / TY; }
                     else if (d == 1) { lL[0] = qq % TX; lL[2] = qq / TX; }
                     else { lL[0] = qq % TX; lL[1] = qq / TX; }
+                    int lR[3] = {lL[0], lL[1], lL[2]};
                     lL[d] = fidx - 1;
-                    lR[0] = lL[0]; lR[1] = lL[1]; lR[2] = lL[2];
                     lR[d] = fidx;
-                    if (D == 2) { lL[2] = 0; lR[2] = 0; }
                     const int gface = o[d] + fidx;
                     const bool ghostL = gface == 0 && G.bc[d] != kPeriodic;
                     const bool ghostR = gface == G.N[d] && G.bc[d] != kPeriodic;
                     double uL[V], uR[V];
                     if (!ghostL) {
-                        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * V * NPT;
+                        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * SS;
 #pragma unroll
                         for (int v = 0; v < V; v++) {
                             double a = 0;
@@ -400,7 +402,7 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                         }
                     }
                     if (!ghostR) {
-                        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * V * NPT;
+                        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * SS;
 #pragma unroll
                         for (int v = 0; v < V; v++) {
                             double a = 0;
@@ -428,16 +430,16 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                     if (fidx >= 1) {
                         c[d] = nf - 1;
                         const int fi = fp_index<n, nf>(d, c);
-                        double* dst = FX + (d * NE + TL::slot(lL[0], lL[1], lL[2])) * V * NFP;
+                        double* dst = FXd + TL::slot(lL[0], lL[1], lL[2]) * V * FXS;
 #pragma unroll
-                        for (int v = 0; v < V; v++) dst[v * NFP + fi] = F[v];
+                        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
                     }
                     if (fidx < Td) {
                         c[d] = 0;
                         const int fi = fp_index<n, nf>(d, c);
-                        double* dst = FX + (d * NE + TL::slot(lR[0], lR[1], lR[2])) * V * NFP;
+                        double* dst = FXd + TL::slot(lR[0], lR[1], lR[2]) * V * FXS;
 #pragma unroll
-                        for (int v = 0; v < V; v++) dst[v * NFP + fi] = F[v];
+                        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
                     }
                 }
             }
@@ -465,12 +467,24 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
 #pragma unroll
                     for (int v = 0; v < V; v++) {
                         double dudt = 0;
+                        if (G.uniform_pow2) {
+                            // every active h is the same power of two: the
+                            // scaling of each term by 1/h is exact and
+                            // commutes with the rounding of the sum
 #pragma unroll
-                        for (int ll = 0; ll < nf; ll++) {
+                            for (int ll = 0; ll < nf; ll++)
 #pragma unroll
-                            for (int d = 0; d < D; d++) {
-                                const double Fv = FX[((d * NE + el) * V + v) * NFP + fpi[d][ll]];
-                                dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], G.h[d], G.rh[d], G.pow2[d] != 0);
+                                for (int d = 0; d < D; d++)
+                                    dudt += FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]] * M.dfp_to_sp[c[d] * nf + ll];
+                            dudt *= G.rh[0];
+                        } else {
+#pragma unroll
+                            for (int ll = 0; ll < nf; ll++) {
+#pragma unroll
+                                for (int d = 0; d < D; d++) {
+                                    const double Fv = FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]];
+                                    dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], G.h[d], G.rh[d], G.pow2[d] != 0);
+                                }
                             }
                         }
                         if (MODE == kPredict) {
@@ -479,7 +493,7 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                                 if (tt == t) dreg[r][v][tt] = dudt;
                         } else {
                             if (G.grav && v != 0) {
-                                const double* uv = Ss + el * V * NPT;
+                                const double* uv = Ss + el * SS;
                                 double s;
                                 if (v <= D) s = uv[pt] * G.g[v - 1];
                                 else {
@@ -499,7 +513,7 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
 #pragma unroll
             for (int d = 0; d < D; d++) {
                 double* out = A.ff[d];
-                const double* Fd = FX + d * NE * V * NFP;
+                const double* Fd = FX + d * NE * V * FXS;
                 if (D == 2) {
                     for (int q = tid; q < NE * V * NFP; q += kThreads) {
                         const int el = q / (V * NFP);
@@ -513,7 +527,7 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
 #pragma unroll
                         for (int m = 0; m < n; m++) {
                             const int src = d == 0 ? (ll + nf * m) : (m + n * ll);
-                            f += Fd[(el * V + v) * NFP + src] * Mc[cc * n + m];
+                            f += Fd[(el * V + v) * FXS + src] * Mc[cc * n + m];
                         }
                         out[(((long long)t * E + sl_elem[el]) * V + v) * NFP + fi] = f;
                     }
@@ -522,7 +536,7 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                     const int d1 = d == 0 ? 1 : (d == 1 ? 2 : 0);
                     const int d2 = d1 == 0 ? 1 : (d1 == 1 ? 2 : 0);
                     for (int q = tid; q < NE * V * NFP; q += kThreads) {
-                        const int base = q - q % NFP;
+                        const int base = (q / NFP) * FXS;
                         const int fi = q % NFP;
                         int c[3];
                         // decode face index of direction d
@@ -699,8 +713,8 @@ template <int D, int P, int TX, int TY, int TZ>
 constexpr size_t picard_smem_bytes() {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
-    size_t a = (size_t)TL::NS * S::V * S::NPT;
-    size_t b = (size_t)D * TL::NE * S::V * S::NFP;
+    size_t a = (size_t)TL::NS * PicardPad<D, P>::SS;
+    size_t b = (size_t)D * TL::NE * S::V * PicardPad<D, P>::FXS;
     size_t c = (size_t)TL::NE * S::V * S::NFP;
     size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
     size_t total = a + b + c;

@@ -110,7 +110,7 @@ KernelSet make_set() {
     k.predict = picard_kernel<D, P, TX, TY, TZ, kPredict>;
     k.correct = picard_kernel<D, P, TX, TY, TZ, kCorrect>;
     k.flux = picard_kernel<D, P, TX, TY, TZ, kFlux>;
-    k.detect = fv_detect_kernel<D, P>;
+    k.detect = fv_detect_kernel<D, P, TX, TY, TZ>;
     k.theta = fv_theta_kernel<D, P, TX, TY, TZ>;
     k.update = fv_update_kernel<D, P, TX, TY, TZ>;
     k.init = init_state_kernel<D, P>;
@@ -126,7 +126,9 @@ KernelSet make_set() {
 // Tile choice: the largest instantiated tile that divides the element counts.
 template <int P>
 bool pick2(int Nx, int Ny, KernelSet* k) {
-    if (P <= 4 && Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
+    if constexpr (P <= 4) {
+        if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
+    }
     if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<2, P, 2, 2, 1>(); return true; }
     *k = make_set<2, P, 1, 1, 1>();
     return true;

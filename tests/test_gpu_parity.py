@@ -152,7 +152,7 @@ def test_trouble_flags_match_oracle():
     o.step(dt)
     g.step()
     g.sync()
-    tr = o.array("troubles")[5, 0, 2:-2, 2:-2]         # (Y, X) aggregate over the active frame
+    tr = o.array("troubles")[5, 0, 2:-2, 2:-2, 0, 0, 0, 0]  # (Y, X) aggregate over the active frame
     n = 4
     tg = g.read(2).reshape(8, 8, n, n).transpose(0, 2, 1, 3).reshape(8 * n, 8 * n)
     assert tr.sum() > 0
