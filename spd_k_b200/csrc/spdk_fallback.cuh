@@ -375,6 +375,7 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
         const int lx = s % TX, ly = (s / TX) % TY, lz = s / (TX * TY);
         el_ge[s] = ((long long)(oe[2] + lz) * G.N[1] + (oe[1] + ly)) * G.N[0] + (oe[0] + lx);
     }
+    __syncthreads();  // el_ge is read by every thread below
     const double dt = *A.dt;
     const double wdt = M.wt[A.t] * dt;
     const long long E = G.E;

@@ -49,6 +49,7 @@ struct spdk_hydro {
     double2 *rpo = nullptr, *rpn = nullptr;
     uint8_t *trouble = nullptr, *theta = nullptr;
     unsigned long long* dtmin = nullptr;
+    int* status = nullptr;  // device-detected faults (kStatus* bits)
     size_t bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -61,6 +62,16 @@ struct spdk_hydro {
 };
 
 namespace {
+
+// device-detected faults: a bounded wait that ran out sets a status bit
+int check_status(spdk_hydro* h) {
+    int st = 0;
+    cudaError_t e = cudaMemcpyAsync(&st, h->status, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("status read: ") + cudaGetErrorString(e));
+    if (st & kStatusStagingTimeout) return fail(1, "a shared-memory staging wait timed out on the device");
+    return 0;
+}
 
 int dalloc(spdk_hydro* h, void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
@@ -110,6 +121,13 @@ int enqueue_step(spdk_hydro* h) {
         A.dt = h->dt;
         const double* in = h->u;
         int in_slices = 1;
+        if (h->nt == 1 && !h->cfg.fallback) {
+            // an RK stage updates U in place, so the stage reads its halo
+            // from a copy (the reference's copy_ader into U_ader_sp)
+            SPDK_CUDA(cudaMemcpyAsync(h->ua[0], h->u, (size_t)h->E * h->V * h->NPT * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, h->stream));
+            in = h->ua[0];
+        }
         // Picard predictor passes (ADER only: nt = p+1)
         for (int it = 0; it + 1 < h->nt; it++) {
             A.ua_in = in;
@@ -193,7 +211,7 @@ void release(spdk_hydro* h) {
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
                     h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
-                    h->rpo, h->rpn, h->trouble, h->theta, h->dtmin};
+                    h->rpo, h->rpn, h->trouble, h->theta, h->dtmin, h->status};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -294,11 +312,16 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     if (!rc && h->nt > 1) {
         rc = dalloc(h, (void**)&h->ua[0], state * h->nt);
         if (!rc) rc = dalloc(h, (void**)&h->ua[1], state * h->nt);
+    } else if (!rc && !c.fallback) {
+        rc = dalloc(h, (void**)&h->ua[0], state);  // RK stage input copy
     }
     if (!rc && h->nstages > 1) rc = dalloc(h, (void**)&h->u0, state);
     if (!rc) rc = dalloc(h, (void**)&h->wcv, state);
     if (!rc) rc = dalloc(h, (void**)&h->dt, sizeof(double) * 2);
     if (!rc) rc = dalloc(h, (void**)&h->dtmin, sizeof(unsigned long long));
+    if (!rc) rc = dalloc(h, (void**)&h->status, sizeof(int));
+    if (!rc && cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset status");
+    G.status = h->status;
     if (!rc && c.fallback) {
         const size_t ffb = (size_t)h->nt * h->E * h->V * (h->NPT / h->n) * h->nf * sizeof(double);
         for (int d = 0; d < D && !rc; d++) rc = dalloc(h, (void**)&h->ff[d], ffb);
@@ -387,7 +410,7 @@ int spdk_hydro_get_dt(spdk_hydro* h, double* dt) {
     if (!h || !dt) return fail(SPDK_E_ARG, "null argument");
     SPDK_CUDA(cudaMemcpyAsync(dt, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return check_status(h);
 }
 
 int spdk_hydro_set_dt(spdk_hydro* h, double dt) {
@@ -453,7 +476,7 @@ int spdk_hydro_profile(spdk_hydro* h, int nsteps, double* ms, long long* launche
 int spdk_hydro_sync(spdk_hydro* h) {
     if (!h) return fail(SPDK_E_ARG, "null argument");
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return check_status(h);
 }
 
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t_out) {

@@ -48,6 +48,7 @@ struct DevGrid {
     long long E;
     const double* fvf[3];  // FV faces in frame indexing (active cell a has faces a+2, a+3)
     const double* fvc[3];  // FV centres in frame indexing
+    int* status;           // device-detected faults (kStatus* bits)
     // fallback settings
     double nad_tol;
     int nad_delta, nad_moore, use_sed, blending;
@@ -270,6 +271,171 @@ __device__ __forceinline__ void fv_candidate(const DevGrid& G, double* const* ff
 }
 
 // ---------------------------------------------------------------------------
+// Bulk asynchronous copies (TMA engine, 1-D cp.async.bulk) into shared memory
+// completing on an mbarrier. Every wait is bounded: on time-out the kernel
+// records kStatusStagingTimeout in *status and carries on, so a lost copy
+// can never hang the device; the host turns the flag into an error.
+// ---------------------------------------------------------------------------
+constexpr int kStatusStagingTimeout = 1;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait on one mbarrier phase; false (and the status flag) on time-out
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* status) {
+    for (int i = 0; i < (1 << 20); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (status) atomicOr(status, kStatusStagingTimeout);
+    return false;
+}
+
+// interior flux point of direction d: interpolation, primitives, Euler flux
+template <int D, int P, int TX, int TY, int TZ, int d>
+__device__ __forceinline__ void picard_interior_item(const DevGrid& G, const DevMats& M, const double* Ss,
+                                                     double* FX, int q) {
+    using S = Shape<D, P>;
+    constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
+    constexpr int NE = TX * TY * TZ;
+    constexpr int SS = PicardPad<D, P>::SS, FXS = PicardPad<D, P>::FXS;
+    const int el = q / ((nf - 2) * NTP);
+    const int rr = q % ((nf - 2) * NTP);
+    const int ll = 1 + rr / NTP, tp = rr % NTP;
+    int c[3] = {0, 0, 0};
+    tp_coords<D, n>(d, tp, c);
+    double u[V], w[V], f[V];
+    const double* src = Ss + el * SS;
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+        double a = 0;
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+            c[d] = l;
+            a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[ll * n + l];
+        }
+        u[v] = a;
+    }
+    primitives<D>(u, w, G.gm);
+    euler_flux<D>(u, w, f, d);
+    c[d] = ll;
+    const int fi = fp_index<n, nf>(d, c);
+    double* dst = FX + (d * NE + el) * V * FXS;
+#pragma unroll
+    for (int v = 0; v < V; v++) dst[v * FXS + fi] = f[v];
+}
+
+// element interface of direction d: both interface states, ghost image at a
+// non-periodic domain edge (src/boundary.cpp:48-113), LLF flux written to
+// the adjacent flux points of the tile's elements
+template <int D, int P, int TX, int TY, int TZ, int d>
+__device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats& M, const double* Ss, double* FX,
+                                                 const int o[3], int q) {
+    using S = Shape<D, P>;
+    using TL = Tile<D, TX, TY, TZ>;
+    constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
+    constexpr int NE = TL::NE;
+    constexpr int SS = PicardPad<D, P>::SS, FXS = PicardPad<D, P>::FXS;
+    constexpr int Td = d == 0 ? TX : (d == 1 ? TY : TZ);
+    constexpr int per = (NE / Td) * NTP;
+    const int fidx = q / per;
+    const int rr = q % per;
+    const int qq = rr / NTP, tp = rr % NTP;
+    int c[3] = {0, 0, 0};
+    tp_coords<D, n>(d, tp, c);
+    int lL[3] = {0, 0, 0};
+    if (d == 0) { lL[1] = qq % TY; lL[2] = qq / TY; }
+    else if (d == 1) { lL[0] = qq % TX; lL[2] = qq / TX; }
+    else { lL[0] = qq % TX; lL[1] = qq / TX; }
+    int lR[3] = {lL[0], lL[1], lL[2]};
+    lL[d] = fidx - 1;
+    lR[d] = fidx;
+    const int gface = o[d] + fidx;
+    const bool ghostL = gface == 0 && G.bc[d] != kPeriodic;
+    const bool ghostR = gface == G.N[d] && G.bc[d] != kPeriodic;
+    double uL[V], uR[V];
+    if (!ghostL) {
+        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * SS;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            double a = 0;
+#pragma unroll
+            for (int l = 0; l < n; l++) {
+                c[d] = l;
+                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[(nf - 1) * n + l];
+            }
+            uL[v] = a;
+        }
+    }
+    if (!ghostR) {
+        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * SS;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+            double a = 0;
+#pragma unroll
+            for (int l = 0; l < n; l++) {
+                c[d] = l;
+                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[l];
+            }
+            uR[v] = a;
+        }
+    }
+    if (ghostL) {
+#pragma unroll
+        for (int v = 0; v < V; v++) uL[v] = uR[v];
+        if (G.bc[d] == kReflective) uL[1 + d] = -uL[1 + d];
+    }
+    if (ghostR) {
+#pragma unroll
+        for (int v = 0; v < V; v++) uR[v] = uL[v];
+        if (G.bc[d] == kReflective) uR[1 + d] = -uR[1 + d];
+    }
+    double F[V];
+    riemann_llf<D>(F, uL, uR, d, G.gm);
+    if (fidx >= 1) {
+        c[d] = nf - 1;
+        const int fi = fp_index<n, nf>(d, c);
+        double* dst = FX + (d * NE + TL::slot(lL[0], lL[1], lL[2])) * V * FXS;
+#pragma unroll
+        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
+    }
+    if (fidx < Td) {
+        c[d] = 0;
+        const int fi = fp_index<n, nf>(d, c);
+        double* dst = FX + (d * NE + TL::slot(lR[0], lR[1], lR[2])) * V * FXS;
+#pragma unroll
+        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Picard pass: interpolation to flux points, Euler fluxes, LLF at element
 // interfaces, flux divergence and the ADER predictor / corrector update,
 // fused so that only U_ader crosses HBM.
@@ -287,11 +453,15 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
     // variable row of the flux-point arrays (FXS) start on different banks
     constexpr int SS = PicardPad<D, P>::SS;
     constexpr int FXS = PicardPad<D, P>::FXS;
-    extern __shared__ double smem[];
-    double* Ss = smem;                       // [NS][SS >= V*NPT]
-    double* FX = Ss + NS * SS;               // [D][NE][V][FXS >= NFP]
+    // element-slice chunks are copied by the TMA engine when they are whole
+    // 16-byte units (V*NPT even); otherwise by plain loads
+    constexpr bool kBulk = (V * NPT) % 2 == 0;
+    extern __shared__ __align__(128) double smem[];
+    double* Sbuf = smem;                     // 2 x [NS][SS >= V*NPT] (double buffer)
+    double* FX = Sbuf + 2 * NS * SS;         // [D][NE][V][FXS >= NFP]
     double* TT = FX + D * NE * V * FXS;      // [NE][V][NFP] face-integral scratch (3D)
     __shared__ long long sl_elem[NS];
+    __shared__ uint64_t bar[2];
 
     const int tid = threadIdx.x;
     int o[3];
@@ -309,6 +479,11 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
         TL::coords(s, l);
         sl_elem[s] = elem_of<D>(G, o, l);
     }
+    if (kBulk && tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
     const double dt = *A.dt;
     const int nt = G.nt;
     const long long E = G.E;
@@ -322,125 +497,60 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
             for (int t = 0; t < NT; t++) dreg[r][v][t] = 0;
 
     __syncthreads();
-    for (int t = 0; t < nt; t++) {
-        // ---- stage slice t of the tile and its face halo ----
-        if (t == 0 || A.in_slices > 1) {
-            const double* src = A.in_slices > 1 ? A.ua_in + (long long)t * E * V * NPT : A.ua_in;
+    // one elected thread issues the bulk copies of slice t into buffer b
+    auto issue = [&](int t, int b) {
+        const double* src = A.in_slices > 1 ? A.ua_in + (long long)t * E * V * NPT : A.ua_in;
+        double* dst = Sbuf + b * NS * SS;
+        if (kBulk) {
+            if (tid == 0) {
+                uint32_t bytes = 0;
+                for (int s = 0; s < NS; s++)
+                    if (sl_elem[s] >= 0) bytes += V * NPT * sizeof(double);
+                fence_proxy_async_smem();
+                mbar_expect_tx(&bar[b], bytes);
+                for (int s = 0; s < NS; s++)
+                    if (sl_elem[s] >= 0)
+                        bulk_g2s(dst + s * SS, src + sl_elem[s] * V * NPT, V * NPT * sizeof(double), &bar[b]);
+            }
+        } else {
             for (int q = tid; q < NS * V * NPT; q += kThreads) {
                 const int s = q / (V * NPT), off = q - s * (V * NPT);
                 const long long ge = sl_elem[s];
-                if (ge >= 0) Ss[s * SS + off] = src[ge * V * NPT + off];
+                if (ge >= 0) dst[s * SS + off] = src[ge * V * NPT + off];
             }
-            __syncthreads();
         }
+    };
+    const bool multi = A.in_slices > 1;
+    issue(0, 0);
+    for (int t = 0; t < nt; t++) {
+        // ---- stage slice t (prefetch t+1 into the other buffer) ----
+        const int b = multi ? (t & 1) : 0;
+        double* Ss = Sbuf + b * NS * SS;
+        if (multi && t + 1 < nt) issue(t + 1, b ^ 1);
+        if (t == 0 || multi) {
+            if (kBulk) mbar_wait_bounded(&bar[b], multi ? ((t >> 1) & 1) : 0, G.status);
+            else if (!multi || t == 0) __syncthreads();
+        }
+        if (!kBulk && multi && t > 0) __syncthreads();
         // ---- phase A: flux-point fluxes of every direction ----
-        // one loop per direction (compile-time d after unrolling): interior
-        // flux points first, then the element interfaces of the tile
-#pragma unroll
-        for (int d = 0; d < D; d++) {
+        // one list: interfaces (the heavier items) first, then interior flux
+        // points; every item runs with a compile-time direction
+        {
             constexpr int NINT = NE * (nf - 2) * NTP;
-            const int Td = TL::T(d);
-            const int per = (NE / Td) * NTP;
-            const int total = NINT + (Td + 1) * per;
-            double* FXd = FX + d * NE * V * FXS;
+            constexpr int NF0 = (TX + 1) * (NE / TX) * NTP;
+            constexpr int NF1 = (TY + 1) * (NE / TY) * NTP;
+            constexpr int NF2 = D == 3 ? (TZ + 1) * (NE / TZ) * NTP : 0;
+            constexpr int NFT = NF0 + NF1 + NF2;
+            constexpr int total = NFT + D * NINT;
             for (int q = tid; q < total; q += kThreads) {
-                int c[3] = {0, 0, 0};
-                if (q < NINT) {
-                    // interior flux point ll of element el
-                    const int el = q / ((nf - 2) * NTP);
-                    const int rr = q % ((nf - 2) * NTP);
-                    const int ll = 1 + rr / NTP, tp = rr % NTP;
-                    tp_coords<D, n>(d, tp, c);
-                    double u[V], w[V], f[V];
-                    const double* src = Ss + el * SS;
-#pragma unroll
-                    for (int v = 0; v < V; v++) {
-                        double a = 0;
-#pragma unroll
-                        for (int l = 0; l < n; l++) {
-                            c[d] = l;
-                            a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[ll * n + l];
-                        }
-                        u[v] = a;
-                    }
-                    primitives<D>(u, w, G.gm);
-                    euler_flux<D>(u, w, f, d);
-                    c[d] = ll;
-                    const int fi = fp_index<n, nf>(d, c);
-                    double* dst = FXd + el * V * FXS;
-#pragma unroll
-                    for (int v = 0; v < V; v++) dst[v * FXS + fi] = f[v];
-                } else {
-                    // element interface fidx of direction d
-                    const int r = q - NINT;
-                    const int fidx = r / per;
-                    const int rr = r % per;
-                    const int qq = rr / NTP, tp = rr % NTP;
-                    tp_coords<D, n>(d, tp, c);
-                    int lL[3] = {0, 0, 0};
-                    if (d == 0) { lL[1] = qq % TY; lL[2] = qq / TY; }
-                    else if (d == 1) { lL[0] = qq % TX; lL[2] = qq / TX; }
-                    else { lL[0] = qq % TX; lL[1] = qq / TX; }
-                    int lR[3] = {lL[0], lL[1], lL[2]};
-                    lL[d] = fidx - 1;
-                    lR[d] = fidx;
-                    const int gface = o[d] + fidx;
-                    const bool ghostL = gface == 0 && G.bc[d] != kPeriodic;
-                    const bool ghostR = gface == G.N[d] && G.bc[d] != kPeriodic;
-                    double uL[V], uR[V];
-                    if (!ghostL) {
-                        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * SS;
-#pragma unroll
-                        for (int v = 0; v < V; v++) {
-                            double a = 0;
-#pragma unroll
-                            for (int l = 0; l < n; l++) {
-                                c[d] = l;
-                                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[(nf - 1) * n + l];
-                            }
-                            uL[v] = a;
-                        }
-                    }
-                    if (!ghostR) {
-                        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * SS;
-#pragma unroll
-                        for (int v = 0; v < V; v++) {
-                            double a = 0;
-#pragma unroll
-                            for (int l = 0; l < n; l++) {
-                                c[d] = l;
-                                a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[l];
-                            }
-                            uR[v] = a;
-                        }
-                    }
-                    // ghost interface state (src/boundary.cpp:48-113)
-                    if (ghostL) {
-#pragma unroll
-                        for (int v = 0; v < V; v++) uL[v] = uR[v];
-                        if (G.bc[d] == kReflective) uL[1 + d] = -uL[1 + d];
-                    }
-                    if (ghostR) {
-#pragma unroll
-                        for (int v = 0; v < V; v++) uR[v] = uL[v];
-                        if (G.bc[d] == kReflective) uR[1 + d] = -uR[1 + d];
-                    }
-                    double F[V];
-                    riemann_llf<D>(F, uL, uR, d, G.gm);
-                    if (fidx >= 1) {
-                        c[d] = nf - 1;
-                        const int fi = fp_index<n, nf>(d, c);
-                        double* dst = FXd + TL::slot(lL[0], lL[1], lL[2]) * V * FXS;
-#pragma unroll
-                        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
-                    }
-                    if (fidx < Td) {
-                        c[d] = 0;
-                        const int fi = fp_index<n, nf>(d, c);
-                        double* dst = FXd + TL::slot(lR[0], lR[1], lR[2]) * V * FXS;
-#pragma unroll
-                        for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
-                    }
+                if (q < NF0) picard_face_item<D, P, TX, TY, TZ, 0>(G, M, Ss, FX, o, q);
+                else if (q < NF0 + NF1) picard_face_item<D, P, TX, TY, TZ, 1>(G, M, Ss, FX, o, q - NF0);
+                else if (D == 3 && q < NFT) picard_face_item<D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
+                else {
+                    const int r = q - NFT;
+                    if (r < NINT) picard_interior_item<D, P, TX, TY, TZ, 0>(G, M, Ss, FX, r);
+                    else if (r < 2 * NINT) picard_interior_item<D, P, TX, TY, TZ, 1>(G, M, Ss, FX, r - NINT);
+                    else picard_interior_item<D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, r - 2 * NINT);
                 }
             }
         }
@@ -619,8 +729,8 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
         }
     } else if (MODE == kCorrect) {
         // ---- corrector / RK stage (src/transforms.cpp:327-374, 252-261) ----
-        double* Wsp = Ss;                  // reuse staging memory: [NE][V][NPT]
-        double* Tmp = Ss + NE * V * NPT;
+        double* Wsp = Sbuf;                // reuse staging memory: [NE][V][NPT]
+        double* Tmp = Sbuf + NE * V * NPT;
 #pragma unroll
         for (int r = 0; r < PPT; r++) {
             const int q = tid + r * kThreads;
@@ -675,8 +785,8 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
         }
     } else {
         // ---- U_cv = sp_to_cv(U) and the slice-0 FV candidate ----
-        double* Ut = Ss;
-        double* Tmp = Ss + NE * V * NPT;
+        double* Ut = Sbuf;
+        double* Tmp = Sbuf + NE * V * NPT;
         for (int q = tid; q < NE * V * NPT; q += kThreads) {
             const int el = q / (V * NPT), off = q % (V * NPT);
             Ut[q] = A.u[sl_elem[el] * V * NPT + off];
@@ -713,7 +823,7 @@ template <int D, int P, int TX, int TY, int TZ>
 constexpr size_t picard_smem_bytes() {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
-    size_t a = (size_t)TL::NS * PicardPad<D, P>::SS;
+    size_t a = 2 * (size_t)TL::NS * PicardPad<D, P>::SS;
     size_t b = (size_t)D * TL::NE * S::V * PicardPad<D, P>::FXS;
     size_t c = (size_t)TL::NE * S::V * S::NFP;
     size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse

@@ -61,6 +61,10 @@ FULL_CASES = {
     "config1_sine2d_32": ["job/fallback=false", "mesh/nx1=32", "mesh/nx2=32", "mesh/nx3=1",
                           "time/tlim=1.0", "output/dt=1.0"],
 }
+# the benchmark workload (2D point blast, NAD+MUSCL, gradfree) at reduced
+# and full size for a few steps; the run ends at 0.999 x steps x dt0 with
+# output clamping, as the reference driver does
+BENCH_CASES = {"bench_blast_64": (64, 12), "bench_blast_256": (256, 10)}
 GOLDENS = {
     "hydro_sd/W_cv_N8p3_1_0.dat": "reference golden: 3D sine wave, N=8, p=3, ADER, t=0.1",
     "induction_fv/B2_cv_N8p3_2_0.dat": "reference golden: 3D induction loop with fallback, t=0.2",
@@ -118,6 +122,26 @@ def main():
             manifest["full_cases"][name] = {"overrides": ov, "output": last, "steps": steps,
                                             "sha256_active_rho_vx_vy_p": hashlib.sha256(act4.tobytes()).hexdigest()}
             print(name, last, steps, flush=True)
+    sys.path.insert(0, ROOT)
+    import bench
+    from oracle import oracle as O
+    for name, (N, steps) in BENCH_CASES.items():
+        ov = bench.workload_overrides(N)
+        dt0 = O.Oracle(O.config_from_params(O.apply_overrides({}, ov))).compute_dt()
+        tend = steps * dt0 * 0.999
+        ov = [x for x in ov if not x.startswith("output/")] + [f"time/tlim={tend!r}", f"output/dt={tend!r}"]
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out, OMP_NUM_THREADS="8")
+            r = subprocess.run([REF_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            raw = np.fromfile(os.path.join(out, f"W_cv_N{N}p3_1_0.dat"))
+            w = raw.reshape(1, 6, 1, N + 2, N + 2, 1, 4, 4)[0, :5, :, 1:-1, 1:-1]
+            a4 = np.ascontiguousarray(w[[0, 1, 2, 4]]) + 0.0   # +0.0 folds signed zeros
+            nsteps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), W_cv=a4)
+            manifest.setdefault("bench_cases", {})[name] = {
+                "overrides": ov, "steps": nsteps, "slots": "rho, vx, vy, p",
+                "sha256_signed_zero_folded": hashlib.sha256(a4.tobytes()).hexdigest()}
+            print(name, nsteps, flush=True)
     for rel, what in GOLDENS.items():
         path = os.path.join(REF_TREE, "tests", "goldens", rel)
         if os.path.exists(path):
