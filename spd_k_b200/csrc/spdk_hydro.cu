@@ -349,10 +349,15 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     }
     if (!rc) {
         const void* fns[] = {(const void*)h->ks.predict, (const void*)h->ks.correct, (const void*)h->ks.flux};
-        for (const void* f : fns)
+        for (const void* f : fns) {
             if (!rc && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)h->ks.picard_smem) != cudaSuccess)
                 rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.picard_smem) + " bytes");
+            // the whole unified L1/shared array as shared memory: residency is
+            // limited by shared memory, not by L1 (staging goes through TMA)
+            if (!rc) cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        }
+        if (!rc) cudaFuncSetAttribute((const void*)h->ks.update, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (!rc && cudaFuncSetAttribute((const void*)h->ks.update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)h->ks.update_smem) != cudaSuccess)
             rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.update_smem) + " bytes");

@@ -441,7 +441,7 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // fused so that only U_ader crosses HBM.
 // ---------------------------------------------------------------------------
 template <int D, int P, int TX, int TY, int TZ, int MODE>
-__global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, PicardArgs A) {
+__global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats M, PicardArgs A) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
@@ -625,21 +625,22 @@ __global__ void __launch_bounds__(kThreads) picard_kernel(DevGrid G, DevMats M, 
                 double* out = A.ff[d];
                 const double* Fd = FX + d * NE * V * FXS;
                 if (D == 2) {
-                    for (int q = tid; q < NE * V * NFP; q += kThreads) {
-                        const int el = q / (V * NFP);
-                        const int rem = q % (V * NFP);
-                        const int v = rem / NFP, fi = rem % NFP;
-                        // fi = (face ll along d, transverse cell c)
+                    for (int q = tid; q < NE * NFP; q += kThreads) {
+                        const int el = q / NFP, fi = q % NFP;
+                        // fi = (face ll along d, transverse cell cc)
                         int ll, cc;
                         if (d == 0) { ll = fi % nf; cc = fi / nf; }
                         else { cc = fi % n; ll = fi / n; }
-                        double f = 0;
+                        double* dst = out + (((long long)t * E + sl_elem[el]) * V) * NFP + fi;
+                        const double* srcb = Fd + el * V * FXS + (d == 0 ? ll : n * ll);
 #pragma unroll
-                        for (int m = 0; m < n; m++) {
-                            const int src = d == 0 ? (ll + nf * m) : (m + n * ll);
-                            f += Fd[(el * V + v) * FXS + src] * Mc[cc * n + m];
+                        for (int v = 0; v < V; v++) {
+                            double f = 0;
+#pragma unroll
+                            for (int m = 0; m < n; m++)
+                                f += srcb[v * FXS + (d == 0 ? nf * m : m)] * Mc[cc * n + m];
+                            dst[v * NFP] = f;
                         }
-                        out[(((long long)t * E + sl_elem[el]) * V + v) * NFP + fi] = f;
                     }
                 } else {
                     // two transverse sweeps: dim1 = next(d), dim2 = next(dim1)
