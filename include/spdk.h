@@ -156,6 +156,26 @@ int spdk_build_matrices(int p, int ader, double* sp_to_fp, double* dfp_to_sp, do
  * [element][var][point]; count = elements * (ndim+2) * points. */
 int spdk_initial_wcv(const spdk_hydro_config* cfg, double* out, size_t count);
 
+/* Allocation-free step. No counterpart in the reference: it serves callers
+ * that cannot allocate device memory when they advance the solution -- a
+ * host that owns all device memory through its own pool, a plugin running
+ * inside a stream capture it does not own, a real-time loop that cannot
+ * absorb the synchronisation an allocation may cause. It runs one ADER or
+ * SSP-RK step without the fallback for configuration cfg on caller-owned
+ * device buffers: u_in / u_out [element][var][point] (may be the same
+ * buffer), wcv_out (nullable) receives W_cv, *dt_inout holds this step's dt
+ * on entry and the next dt on exit; all work is ordered on `stream` (a
+ * cudaStream_t). Working storage is one fixed array inside the library of
+ * SPDK_NOALLOC_SCRATCH_BYTES bytes, held on every GPU that loads the library
+ * until exit; problems that need more (ADER: 2(p+1) states, RK: 2 states)
+ * are rejected with SPDK_E_ARG. The first call on a device, with that device
+ * current, resolves the array's device address and sets kernel attributes:
+ * make it before any stream capture. Calls share the array, so calls that
+ * overlap on the GPU race; order them on one stream. No call allocates. */
+#define SPDK_NOALLOC_SCRATCH_BYTES (16u << 20)
+int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const double* u_in, double* u_out, double* wcv_out,
+                            double* dt_inout, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

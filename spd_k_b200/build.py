@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspdk_cuda.so")
 SOURCES = ["spdk_hydro.cu", "spdk_select_2d_low.cu", "spdk_select_2d_high.cu", "spdk_select_3d.cu",
-           "spdk_setup.cpp", "spdk_host_api.cpp"]
+           "spdk_noalloc.cu", "spdk_setup.cpp", "spdk_host_api.cpp"]
 HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_kernelset.cuh", "spdk_setup.h"]
 
 
