@@ -123,14 +123,15 @@ def peaks():
 # ---------------------------------------------------------------------------
 # algorithmic bytes per launch of each kernel kind (FP64 parity form)
 # ---------------------------------------------------------------------------
-def algorithmic_bytes(info, fallback):
+def algorithmic_bytes(info, fallback, esz=8):
     """Compulsory HBM bytes of one launch of each kernel kind; S = one state
-    array (E x V x NPT doubles)."""
+    array (E x V x NPT values of esz bytes; the (rho, p) candidates and the
+    dt word stay FP64 in both forms)."""
     E, V, npt, nt, D, p = info.n_elements, info.nvar, info.n_points, info.n_time_slices, info.ndim, info.p
     n, nf = p + 1, p + 2
-    S = E * V * npt * 8
+    S = E * V * npt * esz
     cells = E * npt
-    ff_slice = D * E * V * (npt // n) * nf * 8          # FV face fluxes of one slice
+    ff_slice = D * E * V * (npt // n) * nf * esz        # FV face fluxes of one slice
     b = {}
     # predictor: first pass reads U once and writes nt slices; later passes
     # read nt slices + U and write nt slices; averaged over the p passes
@@ -148,13 +149,13 @@ def algorithmic_bytes(info, fallback):
 KINDS = ["predict", "correct", "flux", "detect", "theta", "update", "other"]
 
 
-def traffic_from_profiles(kind):
+def traffic_from_profiles(kind, workload=WORKLOAD):
     """dram bytes per launch of a kernel kind from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
             j = json.load(f)
-        v = j.get(WORKLOAD, {}).get(kind)
+        v = j.get(workload, {}).get(kind)
         return float(v) if v is not None else None
     except Exception:
         return None
@@ -271,6 +272,8 @@ def main():
     ap.add_argument("--N", type=int, default=256)
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the timed steps one by one instead of replaying the step graph")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="arithmetic of the timed form; fp32 also times the plain fp64 form beside it")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -283,7 +286,8 @@ def main():
     import spd_k_b200 as S
     from spd_k_b200.api import _lib
 
-    c = workload_config(args.N)
+    c = dict(workload_config(args.N), precision=args.precision)
+    esz = 4 if args.precision == "fp32" else 8
     solver = S.HydroSolver(c, device=local)
     L = S.load_library()
     info = solver.info
@@ -336,11 +340,11 @@ def main():
     assert rc == 0, _lib.spdk_last_error()
     per_kind = {KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i]),
                            "avg_us": (1e3 * kms[i] / kl[i]) if kl[i] else None} for i in range(7)}
-    alg = algorithmic_bytes(info, c["fallback"])
+    alg = algorithmic_bytes(info, c["fallback"], esz)
     dom = max((k for k in KINDS if k in alg and per_kind[k]["launches"]), key=lambda k: per_kind[k]["ms"])
     hbm, peak_kind = peaks()
     achieved = alg[dom] / (per_kind[dom]["avg_us"] * 1e-6) / 1e9
-    traffic = traffic_from_profiles(dom)
+    traffic = traffic_from_profiles(dom, WORKLOAD if args.precision == "fp64" else f"{WORKLOAD}-{args.precision}")
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes": alg[dom]}
@@ -351,7 +355,7 @@ def main():
     # ---- e2e through the C ABI with host buffers (reference driver loop) ----
     solver2 = S.HydroSolver(c, device=local)
     u_host = torch.empty(info.n_elements * info.nvar * info.n_points, dtype=torch.float64,
-                         pin_memory=True).numpy()
+                         pin_memory=True).numpy()   # the C ABI exchanges doubles in both forms
     solver2.read(S.FIELD_U_SP, out=u_host)
     w_host = torch.empty_like(torch.from_numpy(u_host)).pin_memory().numpy()
     rc = L.spdk_hydro_get_stream(solver2.h, ctypes.byref(sp))
@@ -376,6 +380,28 @@ def main():
            "steps": e2e_steps, "path": "spdk_hydro_write + spdk_hydro_step/get_dt per step + spdk_hydro_read"}
     solver2.close()
 
+    # ---- the plain FP64 form on the same workload, beside the precision form ----
+    plain = None
+    if args.precision != "fp64":
+        c64 = dict(c, precision="fp64")
+        s64 = S.HydroSolver(c64, device=local)
+        rc = L.spdk_hydro_get_stream(s64.h, ctypes.byref(sp))
+        st64 = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
+        s64.steps(args.warmup)
+        s64.sync()
+        barrier(dist)
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(st64)
+        s64.steps(args.steps)
+        g1.record(st64)
+        g1.synchronize()
+        ms64 = max_over_ranks(dist, g0.elapsed_time(g1), f"cuda:{local}")
+        plain = {"value": aggregate_throughput(world, dof, args.steps, ms64), "unit": "DOF-updates/s",
+                 "ms_per_step": ms64 / args.steps, "steps": args.steps,
+                 "speedup": (ms64 / args.steps) / (ms / args.steps)}
+        s64.close()
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -391,12 +417,14 @@ def main():
         line = {
             "metric": "DOF-updates/s", "value": value, "unit": "DOF-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (f64 islands)" if args.precision == "fp32" else "f64",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "elements": [args.N, args.N], "p": 3, "dof_per_gpu": dof,
                        "integrator": "ader", "riemann": "LLF at SD faces, HLLC at fallback faces",
                        "fallback": "NAD(1e-5, Moore)+SED+PAD, theta-blended MUSCL-Hancock",
-                       "precision": "fp64, reference operation order (plain form)",
+                       "precision": ("fp32 state/transforms/fluxes; fp64 pressure recovery, detector bounds, dt"
+                                     if args.precision == "fp32" else "fp64, reference operation order (plain form)"),
                        "parallelism": f"replicas{world}",
                        "l2": f"no flush: device working set {state_gb:.2f} GB > 126 MB L2",
                        "state": "steps continue from the initial blast after the warm-up"},
@@ -404,6 +432,7 @@ def main():
             "roofline": roofline,
             "kernels": kernel_table,
             "e2e": e2e,
+            "plain_fp64": plain,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -53,7 +53,11 @@ enum {
 
 /* arithmetic of the solver */
 enum {
-    SPDK_PRECISION_FP64 = 0   /* plain form: FP64, reference operation order */
+    SPDK_PRECISION_FP64 = 0,  /* plain form: FP64, reference operation order */
+    SPDK_PRECISION_FP32 = 1   /* precision form: FP32 state, transforms and fluxes
+                                 (FMA contraction allowed); FP64 for pressure
+                                 recovery, the detector's bound comparisons and
+                                 the dt reduction. No reference counterpart. */
 };
 
 typedef struct spdk_hydro_config {

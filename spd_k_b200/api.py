@@ -23,6 +23,9 @@ PROBLEMS = {
     "rti_top": 12,
 }
 FIELD_U_SP, FIELD_W_CV, FIELD_TROUBLES, FIELD_THETA = 0, 1, 2, 3
+# arithmetic of the solver: the plain FP64 form (bitwise the reference) or
+# the FP32 precision form (FP64 kept for pressure recovery, detector bounds, dt)
+PRECISIONS = {"fp64": 0, "fp32": 1}
 
 # per-problem <problem> defaults (src/main.cpp:31-65):
 # amp, v1, v2, v3, d0, d1, p0, p1, radius, sigma, dir
@@ -211,7 +214,10 @@ def make_config(c, device=0):
     for i, v in enumerate(c.get("q", [])):
         o.q[i] = v
     o.seed = int(c.get("seed", 0))
-    o.precision = 0
+    prec = c.get("precision", "fp64")
+    if prec not in PRECISIONS:
+        raise ValueError(f"unknown precision {prec!r} ({', '.join(PRECISIONS)})")
+    o.precision = PRECISIONS[prec]
     o.device = device
     return o
 

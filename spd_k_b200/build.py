@@ -2,7 +2,10 @@
 
 The parity (FP64) kernels are compiled with -fmad=false and the host code
 with -ffp-contract=off: no product is fused into a sum anywhere, so the
-arithmetic rounds exactly like the reference's x86-64 CPU build.
+arithmetic rounds exactly like the reference's x86-64 CPU build. The FP32
+precision form's translation units (FP32_SOURCES) are compiled with FMA
+contraction and FP32 division/square root to within 2 ulp (its FP64
+islands are unaffected): that form makes no bitwise claim.
 """
 import os
 import shutil
@@ -14,7 +17,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libspdk_cuda.so")
 SOURCES = ["spdk_hydro.cu", "spdk_select_2d_low.cu", "spdk_select_2d_high.cu", "spdk_select_3d.cu",
+           "spdk_select_f32_2d.cu", "spdk_select_f32_3d.cu",
            "spdk_noalloc.cu", "spdk_setup.cpp", "spdk_host_api.cpp"]
+FP32_SOURCES = {"spdk_select_f32_2d.cu", "spdk_select_f32_3d.cu"}
 HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_kernelset.cuh", "spdk_setup.h"]
 
 
@@ -25,10 +30,11 @@ def nvcc_path():
     raise RuntimeError("nvcc not found")
 
 
-def flags(extra=()):
+def flags(extra=(), fmad=False):
     return [
         "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-        "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+        *(["-fmad=true", "-prec-div=false", "-prec-sqrt=false"] if fmad else ["-fmad=false"]),
+        "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
         "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
         "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills",
         *extra,
@@ -53,7 +59,7 @@ def build(force=False, verbose=False, jobs=None):
     objs, procs = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src + ".o")
-        cmd = [nvcc, *flags(), "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc, *flags(fmad=src in FP32_SOURCES), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         procs.append((subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT), src))

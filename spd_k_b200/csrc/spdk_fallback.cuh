@@ -14,13 +14,13 @@
 
 namespace spdk {
 
-struct FallbackArgs {
-    const double* ucv_in;   // U_cv at the start of slice t [E][V][NPT]
-    double* ucv_out;        // U_cv after slice t
-    double* const* ff;      // FV face fluxes, all slices
-    double* ff0;            // direction arrays (copied for by-value passing)
-    double* ff1;
-    double* ff2;
+template <typename R>
+struct FallbackArgsT {
+    const R* ucv_in;        // U_cv at the start of slice t [E][V][NPT]
+    R* ucv_out;             // U_cv after slice t
+    R* ff0;                 // FV face fluxes of each direction, all slices
+    R* ff1;
+    R* ff2;
     const double2* rp_old;  // (rho, p) of U_old / U_new candidates of slice t
     const double2* rp_new;
     double2* rp_old_next;   // candidates of slice t+1
@@ -29,15 +29,16 @@ struct FallbackArgs {
     uint8_t* theta;         // [E][NPT], theta * 8
     int t;                  // slice
     int last;               // last slice of the stage: U_sp = cv_to_sp(U_cv)
-    double* u;              // U_sp (written on the last slice)
-    const double* u0;       // RK step-start state
+    R* u;                   // U_sp (written on the last slice)
+    const R* u0;            // RK step-start state
     double rk_a;
     int final_stage;        // compute W_cv and the next dt
-    double* wcv;
+    R* wcv;
     unsigned long long* dtmin;
     const double* dt;
     int* any_trouble;       // diagnostic counter of troubled sub-cells (nullable)
 };
+using FallbackArgs = FallbackArgsT<double>;
 
 // active FV cell -> (element, point) index of a [E][NPT] array
 template <int D, int P>
@@ -113,7 +114,10 @@ __device__ __forceinline__ double sed_component(const DevGrid& G, const double2*
     return smin(smin(al[0], al[1]), al[2]);
 }
 
-template <int D, int P, int TX, int TY, int TZ>
+// R names the form (double: plain, float: precision) that launches the
+// kernel; the detector computes in FP64 in both, and a separate
+// instantiation per form keeps each form's compile flags on its own copy.
+template <typename R, int D, int P, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
                                                             uint8_t* __restrict__ T, int* any_trouble) {
@@ -217,7 +221,7 @@ struct CellBox {
 // theta = max over the Moore box of w(#offsets) * trouble, plus the 0.25 ring
 // (src/trouble_detection.cpp:191-242); theta_from_troubles without blending
 // ---------------------------------------------------------------------------
-template <int D, int P, int TX, int TY, int TZ>
+template <typename R, int D, int P, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uint8_t* __restrict__ T,
                                                            uint8_t* __restrict__ theta) {
     constexpr int n = P + 1;
@@ -287,39 +291,39 @@ __global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uin
 // MUSCL-Hancock face states of cell X for a face of direction Dn
 // (src/hydro.cpp:622-681); returns the state on the cell's low face (wlo)
 // and high face (whi). Wc(offset) gives W_old of neighbouring cells.
-template <int D, typename WF>
-__device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], int Dn, double dtw, WF Wc,
-                                           double* wlo, double* whi) {
+template <int D, typename R, typename WF>
+__device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], int Dn, R dtw, WF Wc,
+                                           R* wlo, R* whi) {
     constexpr int V = D + 2;
-    double w[V], dW[D][V], dwt[V];
-    const double* wc = Wc(0, 0, 0);
+    R w[V], dW[D][V], dwt[V];
+    const R* wc = Wc(0, 0, 0);
 #pragma unroll
     for (int v = 0; v < V; v++) w[v] = wc[v];
 #pragma unroll
     for (int d = 0; d < D; d++) {
-        const double* wm = Wc(d == 0 ? -1 : 0, d == 1 ? -1 : 0, d == 2 ? -1 : 0);
-        const double* wp = Wc(d == 0 ? 1 : 0, d == 1 ? 1 : 0, d == 2 ? 1 : 0);
+        const R* wm = Wc(d == 0 ? -1 : 0, d == 1 ? -1 : 0, d == 2 ? -1 : 0);
+        const R* wp = Wc(d == 0 ? 1 : 0, d == 1 ? 1 : 0, d == 2 ? 1 : 0);
         const double* xc = G.fvc[d];
         const double* xf = G.fvf[d];
         const int i = fa[d];
 #pragma unroll
         for (int v = 0; v < V; v++)
-            dW[d][v] = minmod((wp[v] - w[v]) / (xc[i + 1] - xc[i]), (w[v] - wm[v]) / (xc[i] - xc[i - 1]), xf[i],
-                              xf[i + 1]);
+            dW[d][v] = minmod((wp[v] - w[v]) / (R)(xc[i + 1] - xc[i]), (w[v] - wm[v]) / (R)(xc[i] - xc[i - 1]),
+                              (R)xf[i], (R)xf[i + 1]);
     }
-    hancock<D>(w, dwt, dW, G.gm);
+    hancock<D>(w, dwt, dW, (R)G.gm);
     const double* xf = G.fvf[Dn];
     const int i = fa[Dn];
-    const double h = xf[i + 1] - xf[i];
+    const R h = (R)(xf[i + 1] - xf[i]);
 #pragma unroll
     for (int v = 0; v < V; v++) {
-        const double dw = dW[Dn][v];
+        const R dw = dW[Dn][v];
         whi[v] = w[v] + dw + dwt[v] * dtw / h;  // reference "WL": left state of the high face
         wlo[v] = w[v] - dw + dwt[v] * dtw / h;  // reference "WR": right state of the low face
     }
 }
 
-template <int D, int P, int TX, int TY, int TZ>
+template <typename R, int D, int P, int TX, int TY, int TZ>
 struct UpdateSmem {
     static constexpr int n = P + 1, V = D + 2;
     static constexpr int NPT = Shape<D, P>::NPT;
@@ -334,8 +338,8 @@ struct UpdateSmem {
     static constexpr size_t faces = (size_t)(NF0 + NF1 + NF2) * V;
     static constexpr size_t wold = (size_t)E2x * E2y * E2z * V;
     static constexpr size_t epi = 2 * (size_t)NE * V * NPT;
-    static constexpr size_t doubles = faces + (wold > epi ? wold : epi);
-    static constexpr size_t bytes = doubles * sizeof(double) + ((size_t)E1x * E1y * E1z + 15) / 16 * 16;
+    static constexpr size_t reals = faces + (wold > epi ? wold : epi);
+    static constexpr size_t bytes = reals * sizeof(R) + ((size_t)E1x * E1y * E1z + 15) / 16 * 16;
 };
 
 // ---------------------------------------------------------------------------
@@ -344,19 +348,20 @@ struct UpdateSmem {
 // either the next slice's candidate or, after the last slice,
 // U_sp = cv_to_sp(U_cv), the RK combination, W_cv and the next dt.
 // ---------------------------------------------------------------------------
-template <int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats M, FallbackArgs A) {
-    using SM = UpdateSmem<D, P, TX, TY, TZ>;
+template <typename R, int D, int P, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+    using SM = UpdateSmem<R, D, P, TX, TY, TZ>;
     constexpr int n = P + 1, nf = P + 2, V = D + 2, NPT = SM::NPT, NFP = Shape<D, P>::NFP;
     constexpr int Bx = SM::Bx, By = SM::By, Bz = SM::Bz, NC = SM::NC;
     constexpr int E1x = SM::E1x, E1y = SM::E1y, E2x = SM::E2x, E2y = SM::E2y;
-    extern __shared__ double smem[];
-    double* Fs = smem;                                   // faces of the tile, [face][V]
-    double* Wo = Fs + SM::faces;                         // W_old on the tile + 2 halo
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R* smem = reinterpret_cast<R*>(smem_raw);
+    R* Fs = smem;                                   // faces of the tile, [face][V]
+    R* Wo = Fs + SM::faces;                         // W_old on the tile + 2 halo
     uint8_t* th = (uint8_t*)(Wo + (SM::wold > SM::epi ? SM::wold : SM::epi));
     __shared__ long long el_ge[SM::NE];
     const int dz = D == 3 ? 1 : 0;
-    double* const ffd[3] = {A.ff0, A.ff1, A.ff2};
+    R* const ffd[3] = {A.ff0, A.ff1, A.ff2};
 
     int o[3], oe[3];
     {
@@ -376,8 +381,8 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
         el_ge[s] = ((long long)(oe[2] + lz) * G.N[1] + (oe[1] + ly)) * G.N[0] + (oe[0] + lx);
     }
     __syncthreads();  // el_ge is read by every thread below
-    const double dt = *A.dt;
-    const double wdt = M.wt[A.t] * dt;
+    const R dt = (R)(*A.dt);
+    const R wdt = M.wt[A.t] * dt;
     const long long E = G.E;
     // theta on the tile + 1 halo (ghost values are images)
     for (int q = threadIdx.x; q < E1x * E1y * SM::E1z; q += blockDim.x) {
@@ -401,8 +406,8 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
             if (llv < 0) llv = c[d];
             c[d] = llv;
             const int fi = fp_index<n, nf>(d, c);
-            const double* src = ffd[d] + ((long long)A.t * E + el_ge[el]) * V * NFP;
-            double* dst = Fs + (size_t)(fbase[d] + q) * V;
+            const R* src = ffd[d] + ((long long)A.t * E + el_ge[el]) * V * NFP;
+            R* dst = Fs + (size_t)(fbase[d] + q) * V;
 #pragma unroll
             for (int v = 0; v < V; v++) dst[v] = src[v * NFP + fi];
         }
@@ -428,10 +433,10 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
             const long long cid = cell_image<D, P>(G, a, fl);
             const long long ge = cid / NPT;
             const int pt = (int)(cid - ge * NPT);
-            double u[V], w[V];
+            R u[V], w[V];
 #pragma unroll
             for (int v = 0; v < V; v++) u[v] = A.ucv_in[(ge * V + v) * NPT + pt];
-            primitives<D>(u, w, G.gm);
+            primitives<D>(u, w, (R)G.gm);
 #pragma unroll
             for (int d = 0; d < D; d++)
                 if (fl[d]) w[1 + d] = -w[1 + d];
@@ -445,11 +450,11 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
                 int a[3] = {q % ex, (q / ex) % ey, q / (ex * ey)};
                 const int sR = (a[0] + 1) + E1x * ((a[1] + 1) + E1y * (a[2] + dz));
                 const int sL = sR - (d == 0 ? 1 : (d == 1 ? E1x : E1x * E1y));
-                const double tR = th[sR] * 0.125, tL = th[sL] * 0.125;
-                const double tf = smax(tR, tL);
+                const R tR = (R)(th[sR] * 0.125), tL = (R)(th[sL] * 0.125);
+                const R tf = smax(tR, tL);
                 if (!(tf > 0)) continue;
                 // cells L (low) and R (high) of the face; W_old box index
-                double wlo_R[V], whi_R[V], wlo_L[V], whi_L[V];
+                R wlo_R[V], whi_R[V], wlo_L[V], whi_L[V];
                 for (int side = 0; side < 2; side++) {
                     int cb[3] = {a[0] + 2, a[1] + 2, a[2] + 2 * dz};
                     if (side == 0) cb[d] -= 1;
@@ -457,20 +462,20 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
                     fa[0] = o[0] + cb[0] - 2 + 2;
                     fa[1] = o[1] + cb[1] - 2 + 2;
                     fa[2] = o[2] + cb[2] - 2 * dz + 2;
-                    auto Wc = [&](int oi, int oj, int ok) -> const double* {
+                    auto Wc = [&](int oi, int oj, int ok) -> const R* {
                         return Wo + (size_t)((cb[0] + oi) + E2x * ((cb[1] + oj) + E2y * (cb[2] + ok))) * V;
                     };
-                    if (side == 0) muscl_cell<D>(G, fa, d, wdt, Wc, wlo_L, whi_L);
-                    else muscl_cell<D>(G, fa, d, wdt, Wc, wlo_R, whi_R);
+                    if (side == 0) muscl_cell<D, R>(G, fa, d, wdt, Wc, wlo_L, whi_L);
+                    else muscl_cell<D, R>(G, fa, d, wdt, Wc, wlo_R, whi_R);
                 }
-                double uL[V], uR[V], fL[V];
-                conservatives<D>(whi_L, uL, G.gm);
-                conservatives<D>(wlo_R, uR, G.gm);
-                riemann_hllc<D>(fL, uL, uR, d, G.gm);
-                double* F = Fs + (size_t)(fbase[d] + q) * V;
+                R uL[V], uR[V], fL[V];
+                conservatives<D>(whi_L, uL, (R)G.gm);
+                conservatives<D>(wlo_R, uR, (R)G.gm);
+                riemann_hllc<D>(fL, uL, uR, d, (R)G.gm);
+                R* F = Fs + (size_t)(fbase[d] + q) * V;
 #pragma unroll
                 for (int v = 0; v < V; v++) {
-                    double f = F[v];
+                    R f = F[v];
                     f = f + tf * (fL[v] - f);
                     F[v] = f;
                 }
@@ -479,39 +484,39 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
         __syncthreads();
     }
     // corrected sub-cell update
-    double* Ub = Wo;                   // [NE][V][NPT] new U_cv of the tile
-    double* Tmp = Wo + SM::NE * V * NPT;
+    R* Ub = Wo;                   // [NE][V][NPT] new U_cv of the tile
+    R* Tmp = Wo + SM::NE * V * NPT;
     for (int q = threadIdx.x; q < NC; q += blockDim.x) {
         int a[3] = {q % Bx, (q / Bx) % By, q / (Bx * By)};
         const int el = (a[0] / n) + TX * ((a[1] / n) + TY * (a[2] / n));
         int c[3] = {a[0] % n, a[1] % n, a[2] % n};
         const int pt = pt_index<n>(c);
         const long long ge = el_ge[el];
-        double hd[3];
+        R hd[3];
         int fl_[3], fr_[3];
 #pragma unroll
         for (int d = 0; d < D; d++) {
             const long long I = (long long)o[d] + a[d] + 2;
-            hd[d] = G.fvf[d][I + 1] - G.fvf[d][I];
+            hd[d] = (R)(G.fvf[d][I + 1] - G.fvf[d][I]);
             const int ex = Bx + (d == 0), ey = By + (d == 1);
             int lo[3] = {a[0], a[1], a[2]}, hi[3] = {a[0], a[1], a[2]};
             hi[d] += 1;
             fl_[d] = fbase[d] + lo[0] + ex * (lo[1] + ey * lo[2]);
             fr_[d] = fbase[d] + hi[0] + ex * (hi[1] + ey * hi[2]);
         }
-        double un[V];
+        R un[V];
 #pragma unroll
         for (int v = 0; v < V; v++) {
-            const double uold = A.ucv_in[(ge * V + v) * NPT + pt];
-            double F = 0;
+            const R uold = A.ucv_in[(ge * V + v) * NPT + pt];
+            R F = 0;
 #pragma unroll
             for (int d = 0; d < D; d++) F += (Fs[(size_t)fr_[d] * V + v] - Fs[(size_t)fl_[d] * V + v]) / hd[d];
             if (G.grav && v != 0) {
-                double s;
-                if (v <= D) s = un[0] * G.g[v - 1];
+                R s;
+                if (v <= D) s = un[0] * (R)G.g[v - 1];
                 else {
-                    s = un[1] * G.g[0] + un[2] * G.g[1];
-                    if (D == 3) s = s + un[3] * G.g[2];
+                    s = un[1] * (R)G.g[0] + un[2] * (R)G.g[1];
+                    if (D == 3) s = s + un[3] * (R)G.g[2];
                 }
                 F -= s;
             }
@@ -524,53 +529,54 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
         }
         if (!A.last) {
             // candidate of slice t+1 from the new U_cv
-            double uc[V], w[V];
-            fv_candidate<D, P>(G, ffd, A.t + 1, ge, pt, un, M.wt[A.t + 1] * dt, uc);
-            primitives<D>(un, w, G.gm);
-            A.rp_old_next[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
-            primitives<D>(uc, w, G.gm);
-            A.rp_new_next[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
+            R uc[V];
+            fv_candidate<D, P, R>(G, ffd, A.t + 1, ge, pt, un, M.wt[A.t + 1] * dt, uc);
+            A.rp_old_next[ge * NPT + pt] = rho_p_fp64<D>(un, G.gm);
+            A.rp_new_next[ge * NPT + pt] = rho_p_fp64<D>(uc, G.gm);
         }
     }
     if (!A.last) return;
     __syncthreads();
     // U_sp = cv_to_sp(U_cv) (src/hydro_ader.hpp:570)
     {
-        double* bufs[2] = {Tmp, Ub};
-        const double* src = Ub;
+        R* bufs[2] = {Tmp, Ub};
+        const R* src = Ub;
         for (int d = 0; d < D; d++) {
-            double* dst = bufs[d % 2];
-            sweep_smem<D, P>(src, dst, M.cv_to_sp, d, SM::NE * V * NPT);
+            R* dst = bufs[d % 2];
+            sweep_smem<D, P, R>(src, dst, M.cv_to_sp, d, SM::NE * V * NPT);
             __syncthreads();
             src = dst;
         }
-        double* Wsp = (double*)(src == Ub ? Tmp : Ub);
+        R* Wsp = (R*)(src == Ub ? Tmp : Ub);
         for (int q = threadIdx.x; q < SM::NE * NPT; q += blockDim.x) {
             const int el = q / NPT, pt = q % NPT;
             const long long ge = el_ge[el];
-            double u[V];
+            R u[V];
 #pragma unroll
             for (int v = 0; v < V; v++) {
                 const long long gi = (ge * V + v) * NPT + pt;
-                double val = src[(el * V + v) * NPT + pt];
-                if (A.rk_a > 0) val = A.rk_a * A.u0[gi] + (1.0 - A.rk_a) * val;
+                R val = src[(el * V + v) * NPT + pt];
+                if (A.rk_a > 0) {
+                    const R ra = (R)A.rk_a;
+                    val = ra * A.u0[gi] + ((R)1.0 - ra) * val;
+                }
                 u[v] = val;
                 A.u[gi] = val;
             }
             if (A.final_stage) {
-                double w[V];
-                primitives<D>(u, w, G.gm);
+                R w[V];
+                primitives<D>(u, w, (R)G.gm);
 #pragma unroll
                 for (int v = 0; v < V; v++) Wsp[(el * V + v) * NPT + pt] = w[v];
             }
         }
         if (!A.final_stage) return;
         __syncthreads();
-        double* bufs2[2] = {(double*)src, Wsp};
-        const double* s2 = Wsp;
+        R* bufs2[2] = {(R*)src, Wsp};
+        const R* s2 = Wsp;
         for (int d = 0; d < D; d++) {
-            double* dst = bufs2[d % 2];
-            sweep_smem<D, P>(s2, dst, M.sp_to_cv, d, SM::NE * V * NPT);
+            R* dst = bufs2[d % 2];
+            sweep_smem<D, P, R>(s2, dst, M.sp_to_cv, d, SM::NE * V * NPT);
             __syncthreads();
             s2 = dst;
         }
@@ -578,7 +584,7 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMats 
         for (int q = threadIdx.x; q < SM::NE * NPT; q += blockDim.x) {
             const int el = q / NPT, pt = q % NPT;
             const long long ge = el_ge[el];
-            double w[V];
+            R w[V];
 #pragma unroll
             for (int v = 0; v < V; v++) w[v] = s2[(el * V + v) * NPT + pt];
             if (A.wcv)

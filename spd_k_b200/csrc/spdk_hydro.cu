@@ -39,12 +39,19 @@ struct spdk_hydro {
     long long E = 0;
     Matrices mats;
     Axis ax[3];
-    DevMats dm{};
+    int prec = SPDK_PRECISION_FP64;
+    size_t esz = sizeof(double);       // bytes per state value
+    DevMatsT<double> dm64{};
+    DevMatsT<float> dm32{};
     DevGrid G{};
-    KernelSet ks;
+    KernelSetT<double> ks64;           // FP64 kernels (also the FP32 form's set-up)
+    KernelSetT<float> ks32;
+    int tile[3] = {1, 1, 1};
     cudaStream_t stream = nullptr;
-    double *u = nullptr, *ua[2] = {nullptr, nullptr}, *u0 = nullptr, *ucv[2] = {nullptr, nullptr};
-    double *ff[3] = {nullptr, nullptr, nullptr}, *wcv = nullptr, *dt = nullptr;
+    // state buffers hold doubles (plain form) or floats (precision form)
+    void *u = nullptr, *ua[2] = {nullptr, nullptr}, *u0 = nullptr, *ucv[2] = {nullptr, nullptr};
+    void *ff[3] = {nullptr, nullptr, nullptr}, *wcv = nullptr;
+    double* dt = nullptr;
     double *fvf[3] = {nullptr, nullptr, nullptr}, *fvc[3] = {nullptr, nullptr, nullptr};
     double2 *rpo = nullptr, *rpn = nullptr;
     uint8_t *trouble = nullptr, *theta = nullptr;
@@ -102,64 +109,66 @@ void prof_end(spdk_hydro* h, int kind) {
 
 unsigned grid_blocks(const spdk_hydro* h) {
     long long b = 1;
-    for (int d = 0; d < h->D; d++) b *= h->G.N[d] / h->ks.tile[d];
+    for (int d = 0; d < h->D; d++) b *= h->G.N[d] / h->tile[d];
     return (unsigned)b;
 }
 
 // launches of one step, recorded on h->stream (also used for capture)
-int enqueue_step(spdk_hydro* h) {
-    const KernelSet& k = h->ks;
+template <typename R>
+int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm) {
     const unsigned blocks = grid_blocks(h);
     int launches = 0;
+    R* const ua[2] = {(R*)h->ua[0], (R*)h->ua[1]};
+    R* const ucv[2] = {(R*)h->ucv[0], (R*)h->ucv[1]};
     if (h->nstages > 1)
-        SPDK_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)h->E * h->V * h->NPT * sizeof(double),
+        SPDK_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)h->E * h->V * h->NPT * sizeof(R),
                                   cudaMemcpyDeviceToDevice, h->stream));
     for (int s = 0; s < h->nstages; s++) {
         const bool final_stage = s == h->nstages - 1;
-        PicardArgs A{};
-        A.u = h->u;
+        PicardArgsT<R> A{};
+        A.u = (const R*)h->u;
         A.dt = h->dt;
-        const double* in = h->u;
+        const R* in = (const R*)h->u;
         int in_slices = 1;
         if (h->nt == 1 && !h->cfg.fallback) {
             // an RK stage updates U in place, so the stage reads its halo
             // from a copy (the reference's copy_ader into U_ader_sp)
-            SPDK_CUDA(cudaMemcpyAsync(h->ua[0], h->u, (size_t)h->E * h->V * h->NPT * sizeof(double),
+            SPDK_CUDA(cudaMemcpyAsync(h->ua[0], h->u, (size_t)h->E * h->V * h->NPT * sizeof(R),
                                       cudaMemcpyDeviceToDevice, h->stream));
-            in = h->ua[0];
+            in = ua[0];
         }
         // Picard predictor passes (ADER only: nt = p+1)
         for (int it = 0; it + 1 < h->nt; it++) {
             A.ua_in = in;
             A.in_slices = in_slices;
-            A.ua_out = h->ua[it % 2];
+            A.ua_out = ua[it % 2];
             prof_begin(h);
-            k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
             prof_end(h, SPDK_KERNEL_PREDICT);
             launches++;
-            in = h->ua[it % 2];
+            in = ua[it % 2];
             in_slices = h->nt;
         }
         A.ua_in = in;
         A.in_slices = in_slices;
         if (!h->cfg.fallback) {
-            A.u_out = h->u;
-            A.u0 = h->u0;
+            A.u_out = (R*)h->u;
+            A.u0 = (const R*)h->u0;
             A.rk_a = h->rk_a[s];
             A.final_stage = final_stage;
-            A.wcv = h->wcv;
+            A.wcv = (R*)h->wcv;
             A.dtmin = h->dtmin;
             prof_begin(h);
-            k.correct<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            k.correct<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
             prof_end(h, SPDK_KERNEL_CORRECT);
             launches++;
         } else {
-            for (int d = 0; d < 3; d++) A.ff[d] = h->ff[d];
-            A.ucv = h->ucv[0];
+            for (int d = 0; d < 3; d++) A.ff[d] = (R*)h->ff[d];
+            A.ucv = ucv[0];
             A.rp_old = h->rpo;
             A.rp_new = h->rpn;
             prof_begin(h);
-            k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, h->dm, A);
+            k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
             prof_end(h, SPDK_KERNEL_FLUX);
             launches++;
             for (int t = 0; t < h->nt; t++) {
@@ -169,12 +178,12 @@ int enqueue_step(spdk_hydro* h) {
                 prof_begin(h);
                 k.theta<<<blocks, kThreads, 0, h->stream>>>(h->G, h->trouble, h->theta);
                 prof_end(h, SPDK_KERNEL_THETA);
-                FallbackArgs F{};
-                F.ucv_in = h->ucv[t % 2];
-                F.ucv_out = h->ucv[(t + 1) % 2];
-                F.ff0 = h->ff[0];
-                F.ff1 = h->ff[1];
-                F.ff2 = h->ff[2];
+                FallbackArgsT<R> F{};
+                F.ucv_in = ucv[t % 2];
+                F.ucv_out = ucv[(t + 1) % 2];
+                F.ff0 = (R*)h->ff[0];
+                F.ff1 = (R*)h->ff[1];
+                F.ff2 = (R*)h->ff[2];
                 F.rp_old = h->rpo;
                 F.rp_new = h->rpn;
                 F.rp_old_next = h->rpo;
@@ -183,15 +192,15 @@ int enqueue_step(spdk_hydro* h) {
                 F.theta = h->theta;
                 F.t = t;
                 F.last = t == h->nt - 1;
-                F.u = h->u;
-                F.u0 = h->u0;
+                F.u = (R*)h->u;
+                F.u0 = (const R*)h->u0;
                 F.rk_a = h->rk_a[s];
                 F.final_stage = final_stage;
-                F.wcv = h->wcv;
+                F.wcv = (R*)h->wcv;
                 F.dtmin = h->dtmin;
                 F.dt = h->dt;
                 prof_begin(h);
-                k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, h->dm, F);
+                k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, dm, F);
                 prof_end(h, SPDK_KERNEL_UPDATE);
                 launches += 3;
             }
@@ -203,6 +212,34 @@ int enqueue_step(spdk_hydro* h) {
     launches++;
     h->launches = launches;
     SPDK_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int enqueue_step(spdk_hydro* h) {
+    return h->prec == SPDK_PRECISION_FP32 ? enqueue_step_t<float>(h, h->ks32, h->dm32)
+                                          : enqueue_step_t<double>(h, h->ks64, h->dm64);
+}
+
+__global__ void narrow_kernel(const double* __restrict__ a, float* __restrict__ b, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// per-kernel attributes: dynamic shared memory and the full carveout
+template <typename R>
+int set_attributes(const KernelSetT<R>& ks) {
+    const void* fns[] = {(const void*)ks.predict, (const void*)ks.correct, (const void*)ks.flux};
+    for (const void* f : fns) {
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ks.picard_smem) != cudaSuccess)
+            return fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(ks.picard_smem) + " bytes");
+        // the whole unified L1/shared array as shared memory: residency is
+        // limited by shared memory, not by L1 (staging goes through TMA)
+        cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+    cudaFuncSetAttribute((const void*)ks.update, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (cudaFuncSetAttribute((const void*)ks.update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ks.update_smem) != cudaSuccess)
+        return fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(ks.update_smem) + " bytes");
     return 0;
 }
 
@@ -234,7 +271,8 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     if (D == 3 && c.p > 5) return fail(SPDK_E_ARG, "3D runs support p <= 5");
     if (D == 2 && (c.g[2] != 0.0 || ((c.problem == SPDK_IC_SINE_WAVE || c.problem == SPDK_IC_SQUARE) && c.v3 != 0.0)))
         return fail(SPDK_E_ARG, "a 2D run cannot carry z momentum or z gravity");
-    if (c.precision != SPDK_PRECISION_FP64) return fail(SPDK_E_ARG, "unsupported precision");
+    if (c.precision != SPDK_PRECISION_FP64 && c.precision != SPDK_PRECISION_FP32)
+        return fail(SPDK_E_ARG, "unsupported precision");
     for (int d = 0; d < D; d++)
         if (c.bc[d] < 0 || c.bc[d] > 2) return fail(SPDK_E_ARG, "bad boundary type");
     if (c.integrator == SPDK_INTEGRATOR_RK && (c.rk_order < 1 || c.rk_order > 3))
@@ -257,27 +295,37 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         if (c.rk_order == 3) { h->rk_a[1] = 0.75; h->rk_a[2] = 1.0 / 3.0; }
     }
     int N[3] = {c.N[0], c.N[1], D == 3 ? c.N[2] : 1};
-    if (!select_kernels(D, c.p, N, &h->ks)) {
+    h->prec = c.precision;
+    h->esz = h->prec == SPDK_PRECISION_FP32 ? sizeof(float) : sizeof(double);
+    if (!select_kernels(D, c.p, N, &h->ks64) ||
+        (h->prec == SPDK_PRECISION_FP32 && !select_kernels(D, c.p, N, &h->ks32))) {
         delete h;
         return fail(SPDK_E_ARG, "no kernel instantiation for this ndim/p");
     }
+    for (int d = 0; d < 3; d++) h->tile[d] = h->ks64.tile[d];
     int rc = cudaSetDevice(c.device) == cudaSuccess ? 0 : fail(SPDK_E_CUDA, "cudaSetDevice failed");
     if (rc) { delete h; return rc; }
     build_matrices(c.p, ader, &h->mats);
     for (int d = 0; d < 3; d++) build_axis(N[d], c.p, c.L[d], h->mats.x_fp, d < D, &h->ax[d]);
     // device matrices (same values as the host setup)
     const int n = h->n, nf = h->nf;
-    std::memset(&h->dm, 0, sizeof(h->dm));
+    std::memset(&h->dm64, 0, sizeof(h->dm64));
     for (int j = 0; j < nf; j++)
-        for (int i = 0; i < n; i++) h->dm.sp_to_fp[j * n + i] = h->mats.sp_to_fp[j * n + i];
+        for (int i = 0; i < n; i++) h->dm64.sp_to_fp[j * n + i] = h->mats.sp_to_fp[j * n + i];
     for (int j = 0; j < n; j++)
-        for (int i = 0; i < nf; i++) h->dm.dfp_to_sp[j * nf + i] = h->mats.dfp_to_sp[j * nf + i];
+        for (int i = 0; i < nf; i++) h->dm64.dfp_to_sp[j * nf + i] = h->mats.dfp_to_sp[j * nf + i];
     for (int q = 0; q < n * n; q++) {
-        h->dm.sp_to_cv[q] = h->mats.sp_to_cv[q];
-        h->dm.cv_to_sp[q] = h->mats.cv_to_sp[q];
+        h->dm64.sp_to_cv[q] = h->mats.sp_to_cv[q];
+        h->dm64.cv_to_sp[q] = h->mats.cv_to_sp[q];
     }
-    for (int q = 0; q < h->nt * h->nt; q++) h->dm.invader[q] = h->mats.invader[q];
-    for (int q = 0; q < h->nt; q++) h->dm.wt[q] = h->mats.wt[q];
+    for (int q = 0; q < h->nt * h->nt; q++) h->dm64.invader[q] = h->mats.invader[q];
+    for (int q = 0; q < h->nt; q++) h->dm64.wt[q] = h->mats.wt[q];
+    {
+        // the precision form's matrices: the FP64 values rounded once
+        const double* src = (const double*)&h->dm64;
+        float* dst = (float*)&h->dm32;
+        for (size_t q = 0; q < sizeof(h->dm64) / sizeof(double); q++) dst[q] = (float)src[q];
+    }
     // grid
     DevGrid& G = h->G;
     h->E = (long long)N[0] * N[1] * N[2];
@@ -305,7 +353,8 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     G.use_sed = (c.sed && c.p > 1) ? 1 : 0;
     G.blending = c.blending;
 
-    const size_t state = (size_t)h->E * h->V * h->NPT * sizeof(double);
+    const size_t state = (size_t)h->E * h->V * h->NPT * h->esz;
+    const size_t state64 = (size_t)h->E * h->V * h->NPT * sizeof(double);
     rc = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess
              ? 0 : fail(SPDK_E_CUDA, "cudaStreamCreate failed");
     if (!rc) rc = dalloc(h, (void**)&h->u, state);
@@ -323,7 +372,7 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     if (!rc && cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset status");
     G.status = h->status;
     if (!rc && c.fallback) {
-        const size_t ffb = (size_t)h->nt * h->E * h->V * (h->NPT / h->n) * h->nf * sizeof(double);
+        const size_t ffb = (size_t)h->nt * h->E * h->V * (h->NPT / h->n) * h->nf * h->esz;
         for (int d = 0; d < D && !rc; d++) rc = dalloc(h, (void**)&h->ff[d], ffb);
         if (!rc) rc = dalloc(h, (void**)&h->ucv[0], state);
         if (!rc) rc = dalloc(h, (void**)&h->ucv[1], state);
@@ -347,35 +396,36 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
             rc = fail(SPDK_E_CUDA, "memset");
         if (!rc && cudaMemset(h->theta, 0, (size_t)h->E * h->NPT) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset");
     }
+    if (!rc) rc = h->prec == SPDK_PRECISION_FP32 ? set_attributes(h->ks32) : set_attributes(h->ks64);
     if (!rc) {
-        const void* fns[] = {(const void*)h->ks.predict, (const void*)h->ks.correct, (const void*)h->ks.flux};
-        for (const void* f : fns) {
-            if (!rc && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)h->ks.picard_smem) != cudaSuccess)
-                rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.picard_smem) + " bytes");
-            // the whole unified L1/shared array as shared memory: residency is
-            // limited by shared memory, not by L1 (staging goes through TMA)
-            if (!rc) cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        }
-        if (!rc) cudaFuncSetAttribute((const void*)h->ks.update, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (!rc && cudaFuncSetAttribute((const void*)h->ks.update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)h->ks.update_smem) != cudaSuccess)
-            rc = fail(SPDK_E_CUDA, "shared memory request of " + std::to_string(h->ks.update_smem) + " bytes");
-    }
-    if (!rc) {
-        // initial condition on the host (transcendentals through the same libm as the reference)
+        // initial condition on the host (transcendentals through the same
+        // libm as the reference), U_sp and dt on the device in FP64; the
+        // precision form starts from that state rounded once to FP32
         std::vector<double> w0;
         initial_wcv(c, h->mats, h->ax, D, &w0);
-        if (cudaMemcpy(h->wcv, w0.data(), state, cudaMemcpyHostToDevice) != cudaSuccess)
+        double *w64 = nullptr, *u64 = nullptr;
+        if (cudaMalloc((void**)&w64, state64) != cudaSuccess || cudaMalloc((void**)&u64, state64) != cudaSuccess)
+            rc = fail(SPDK_E_NOMEM, "set-up buffers");
+        if (!rc && cudaMemcpy(w64, w0.data(), state64, cudaMemcpyHostToDevice) != cudaSuccess)
             rc = fail(SPDK_E_CUDA, "upload W_cv");
-    }
-    if (!rc) {
-        const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
-        cudaMemcpy(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice);
-        h->ks.init<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm, h->wcv, h->u, h->dtmin);
-        advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
-        cudaError_t e = cudaStreamSynchronize(h->stream);
-        if (e != cudaSuccess) rc = fail(SPDK_E_CUDA, std::string("init: ") + cudaGetErrorString(e));
+        if (!rc) {
+            const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+            cudaMemcpy(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice);
+            h->ks64.init<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm64, w64, u64, h->dtmin);
+            advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+            const long long nv = h->E * h->V * h->NPT;
+            if (h->prec == SPDK_PRECISION_FP32) {
+                narrow_kernel<<<1024, 256, 0, h->stream>>>(u64, (float*)h->u, nv);
+                narrow_kernel<<<1024, 256, 0, h->stream>>>(w64, (float*)h->wcv, nv);
+            } else {
+                cudaMemcpyAsync(h->u, u64, state64, cudaMemcpyDeviceToDevice, h->stream);
+                cudaMemcpyAsync(h->wcv, w64, state64, cudaMemcpyDeviceToDevice, h->stream);
+            }
+            cudaError_t e = cudaStreamSynchronize(h->stream);
+            if (e != cudaSuccess) rc = fail(SPDK_E_CUDA, std::string("init: ") + cudaGetErrorString(e));
+        }
+        if (w64) cudaFree(w64);
+        if (u64) cudaFree(u64);
     }
     if (rc) {
         release(h);
@@ -520,8 +570,16 @@ int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count) {
     const size_t cells = (size_t)h->E * h->NPT;
     if (field == SPDK_FIELD_U_SP || field == SPDK_FIELD_W_CV) {
         if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
-        SPDK_CUDA(cudaMemcpyAsync(host, field == SPDK_FIELD_U_SP ? h->u : h->wcv, state * sizeof(double),
-                                  cudaMemcpyDeviceToHost, h->stream));
+        const void* src = field == SPDK_FIELD_U_SP ? h->u : h->wcv;
+        if (h->prec == SPDK_PRECISION_FP32) {
+            // FP32 values widened exactly to doubles
+            std::vector<float> b(state);
+            SPDK_CUDA(cudaMemcpyAsync(b.data(), src, state * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+            SPDK_CUDA(cudaStreamSynchronize(h->stream));
+            for (size_t q = 0; q < state; q++) host[q] = b[q];
+            return 0;
+        }
+        SPDK_CUDA(cudaMemcpyAsync(host, src, state * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         SPDK_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     }
@@ -543,10 +601,24 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     const size_t state = (size_t)h->E * h->V * h->NPT;
     if (field != SPDK_FIELD_U_SP) return fail(SPDK_E_ARG, "only U_sp can be written");
     if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
-    SPDK_CUDA(cudaMemcpyAsync(h->u, host, state * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+    if (h->prec == SPDK_PRECISION_FP32) {
+        // doubles rounded once to FP32
+        std::vector<float> b(host, host + state);
+        SPDK_CUDA(cudaMemcpyAsync(h->u, b.data(), state * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
+        h->ks32.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm32, (const float*)h->u,
+                                                                    (float*)h->wcv, h->dtmin);
+        advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+        SPDK_CUDA(cudaGetLastError());
+        // the pageable staging vector must outlive the copy
+        SPDK_CUDA(cudaStreamSynchronize(h->stream));
+        return 0;
+    }
+    SPDK_CUDA(cudaMemcpyAsync(h->u, host, state * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
-    h->ks.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm, h->u, h->wcv, h->dtmin);
+    h->ks64.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm64, (const double*)h->u,
+                                                                (double*)h->wcv, h->dtmin);
     advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
     SPDK_CUDA(cudaGetLastError());
     SPDK_CUDA(cudaStreamSynchronize(h->stream));

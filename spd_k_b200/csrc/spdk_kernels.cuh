@@ -1,6 +1,6 @@
 // Fused device kernels of the spd_K B200 hydro step.
 //
-// State layout (device, FP64, no ghost elements):
+// State layout (device, arithmetic type R = double or float, no ghost elements):
 //   U, U_cv          [element][var][point]            V = D+2 slots
 //   U_ader (A and B) [slice][element][var][point]     ping-pong per Picard pass
 //   FF_d             [slice][element][var][face point] FV face fluxes of direction d,
@@ -25,15 +25,18 @@ constexpr int kThreads = 256;
 constexpr int kMaxNd = 8;    // n = p+1 <= 8
 constexpr int kMaxNfd = 9;
 
-// Transform matrices, passed by value (kernel parameter space)
-struct DevMats {
-    double sp_to_fp[kMaxNfd * kMaxNd];   // [nf][n]
-    double dfp_to_sp[kMaxNd * kMaxNfd];  // [n][nf]
-    double sp_to_cv[kMaxNd * kMaxNd];    // [n][n]
-    double cv_to_sp[kMaxNd * kMaxNd];
-    double invader[kMaxNd * kMaxNd];     // [nt][nt]
-    double wt[kMaxNd];
+// Transform matrices in the arithmetic type R, passed by value (kernel
+// parameter space). R = double is the plain form; R = float the precision form.
+template <typename R>
+struct DevMatsT {
+    R sp_to_fp[kMaxNfd * kMaxNd];   // [nf][n]
+    R dfp_to_sp[kMaxNd * kMaxNfd];  // [n][nf]
+    R sp_to_cv[kMaxNd * kMaxNd];    // [n][n]
+    R cv_to_sp[kMaxNd * kMaxNd];
+    R invader[kMaxNd * kMaxNd];     // [nt][nt]
+    R wt[kMaxNd];
 };
+using DevMats = DevMatsT<double>;
 
 struct DevGrid {
     int N[3];
@@ -56,23 +59,25 @@ struct DevGrid {
 
 enum { kPredict = 0, kCorrect = 1, kFlux = 2 };
 
-struct PicardArgs {
-    const double* ua_in;   // [slice][E][V][NPT], or U when in_slices == 1
+template <typename R>
+struct PicardArgsT {
+    const R* ua_in;        // [slice][E][V][NPT], or U when in_slices == 1
     int in_slices;         // 1: every slice equals U (first Picard pass / RK stage)
-    const double* u;       // U_sp
-    double* ua_out;        // kPredict output
-    double* u_out;         // kCorrect output (may alias u: element-local)
-    const double* u0;      // RK step-start state
+    const R* u;            // U_sp
+    R* ua_out;             // kPredict output
+    R* u_out;              // kCorrect output (may alias u: element-local)
+    const R* u0;           // RK step-start state
     double rk_a;           // RK convex weight (0: none)
-    double* ff[3];         // kFlux: FV face fluxes, all slices
-    double* ucv;           // kFlux: U_cv = sp_to_cv(U)
-    double2* rp_old;       // kFlux: slice-0 candidate (rho, p) of U_old
-    double2* rp_new;       // kFlux: slice-0 candidate (rho, p) of U_new
-    double* wcv;           // kCorrect: W_cv output (nullable)
+    R* ff[3];              // kFlux: FV face fluxes, all slices
+    R* ucv;                // kFlux: U_cv = sp_to_cv(U)
+    double2* rp_old;       // kFlux: slice-0 candidate (rho, p) of U_old, FP64
+    double2* rp_new;       // kFlux: slice-0 candidate (rho, p) of U_new, FP64
+    R* wcv;                // kCorrect: W_cv output (nullable)
     unsigned long long* dtmin;  // kCorrect: next-dt reduction
     int final_stage;       // kCorrect: compute W_cv and dt
     const double* dt;      // device dt of this step
 };
+using PicardArgs = PicardArgsT<double>;
 
 template <int D, int P>
 struct Shape {
@@ -84,13 +89,18 @@ struct Shape {
     static constexpr int NFP = NTP * nf;   // flux points per direction
 };
 
-// padded shared-memory strides of the Picard pass (bank spreading)
-template <int D, int P>
+// padded shared-memory strides of the Picard pass (bank spreading); an
+// element block (SS) starts on a 16-byte boundary whenever its data is a
+// whole number of 16-byte units, so it can be a bulk-copy destination
+template <int D, int P, typename R = double>
 struct PicardPad {
     static constexpr int V = D + 2;
     static constexpr int NPT = D == 2 ? (P + 1) * (P + 1) : (P + 1) * (P + 1) * (P + 1);
     static constexpr int NFP = NPT / (P + 1) * (P + 2);
-    static constexpr int SS = V * NPT + ((V * NPT) % 32 == 0 ? 2 : 0);
+    static constexpr int Q = 16 / (int)sizeof(R);                   // elements per 16 bytes
+    static constexpr int WORDS = (int)sizeof(R) / 4;                 // 4-byte banks per element
+    static constexpr int SS0 = (V * NPT + Q - 1) / Q * Q;
+    static constexpr int SS = SS0 + ((SS0 * WORDS) % 32 == 0 ? Q : 0);
     static constexpr int FXS = NFP + ((NFP * V) % 16 == 0 ? 1 : 0);
 };
 
@@ -175,9 +185,13 @@ __device__ __forceinline__ long long elem_of(const DevGrid& G, const int o[3], c
     return ((long long)g[2] * G.N[1] + g[1]) * G.N[0] + g[0];
 }
 
-// dt candidate of one W_cv point (src/hydro.cpp:222-254, inviscid)
-template <int D>
-__device__ __forceinline__ double point_dt(const DevGrid& G, const double* w, int n) {
+// dt candidate of one W_cv point (src/hydro.cpp:222-254, inviscid), always
+// evaluated in FP64
+template <int D, typename R>
+__device__ __forceinline__ double point_dt(const DevGrid& G, const R* wr, int n) {
+    double w[D + 2];
+#pragma unroll
+    for (int v = 0; v < D + 2; v++) w[v] = (double)wr[v];
     const double cs = sound_speed(w[0], w[D + 1], G.gm);
     double cmax = 0, dxmin = 1;
 #pragma unroll
@@ -205,8 +219,8 @@ __device__ __forceinline__ void block_min_dt(double v, unsigned long long* out) 
 
 // One directional sweep of element-local arrays in shared memory
 // (src/transforms.cpp:120-147): out(c) = sum_l in(c with c_d = l) * M(c_d, l)
-template <int D, int P>
-__device__ __forceinline__ void sweep_smem(const double* in, double* out, const double* M, int d, int count) {
+template <int D, int P, typename R>
+__device__ __forceinline__ void sweep_smem(const R* in, R* out, const R* M, int d, int count) {
     using S = Shape<D, P>;
     constexpr int n = S::n;
     for (int q = threadIdx.x; q < count; q += blockDim.x) {
@@ -214,7 +228,7 @@ __device__ __forceinline__ void sweep_smem(const double* in, double* out, const 
         int c[3];
         pt_coords<n>(pt, c);
         const int id = c[d];
-        double u = 0;
+        R u = 0;
 #pragma unroll
         for (int l = 0; l < n; l++) {
             c[d] = l;
@@ -227,9 +241,9 @@ __device__ __forceinline__ void sweep_smem(const double* in, double* out, const 
 // Sub-cell candidate of the FV update (src/transforms.cpp:483-543 with
 // update=0): U_new = U_old - (w_t dt) sum_d (F_{+} - F_{-}) / h_d for the
 // cell at point pt of element ge; F from FF_d of slice t.
-template <int D, int P>
-__device__ __forceinline__ void fv_candidate(const DevGrid& G, double* const* ff, int t, long long ge, int pt,
-                                             const double* uold, double wdt, double* unew) {
+template <int D, int P, typename R>
+__device__ __forceinline__ void fv_candidate(const DevGrid& G, R* const* ff, int t, long long ge, int pt,
+                                             const R* uold, R wdt, R* unew) {
     using S = Shape<D, P>;
     constexpr int n = S::n, nf = S::nf, V = S::V;
     int c[3];
@@ -238,12 +252,12 @@ __device__ __forceinline__ void fv_candidate(const DevGrid& G, double* const* ff
     eg[0] = ge % G.N[0];
     eg[1] = (ge / G.N[0]) % G.N[1];
     eg[2] = ge / ((long long)G.N[0] * G.N[1]);
-    double hd[3];
+    R hd[3];
     int fl[3], fr[3];
 #pragma unroll
     for (int d = 0; d < D; d++) {
         const long long I = eg[d] * n + c[d] + 2;
-        hd[d] = G.fvf[d][I + 1] - G.fvf[d][I];
+        hd[d] = (R)(G.fvf[d][I + 1] - G.fvf[d][I]);
         int cc[3] = {c[0], c[1], c[2]};
         fl[d] = fp_index<n, nf>(d, cc);
         cc[d] = c[d] + 1;
@@ -251,23 +265,43 @@ __device__ __forceinline__ void fv_candidate(const DevGrid& G, double* const* ff
     }
 #pragma unroll
     for (int v = 0; v < V; v++) {
-        double F = 0;
+        R F = 0;
 #pragma unroll
         for (int d = 0; d < D; d++) {
-            const double* f = ff[d] + (((long long)t * G.E + ge) * V + v) * S::NFP;
+            const R* f = ff[d] + (((long long)t * G.E + ge) * V + v) * S::NFP;
             F += (f[fr[d]] - f[fl[d]]) / hd[d];
         }
         if (G.grav) {
-            double s = 0;
-            if (v >= 1 && v <= D) s = uold[0] * G.g[v - 1];
+            R s = 0;
+            if (v >= 1 && v <= D) s = uold[0] * (R)G.g[v - 1];
             else if (v == D + 1) {
-                s = uold[1] * G.g[0] + uold[2] * G.g[1];
-                if (D == 3) s = s + uold[3] * G.g[2];
+                s = uold[1] * (R)G.g[0] + uold[2] * (R)G.g[1];
+                if (D == 3) s = s + uold[3] * (R)G.g[2];
             }
             if (v != 0) F -= s;
         }
         unew[v] = uold[v] - wdt * F;
     }
+}
+
+// (rho, p) of a conserved state with the pressure recovered in FP64
+// (src/hydro.cpp:95-106); for R = double these are primitives()'s operations
+template <int D, typename R>
+__device__ __forceinline__ double2 rho_p_fp64(const R* u, double gm) {
+    const double r = (double)u[0];
+    if constexpr (sizeof(R) == 4) {
+        double m2 = 0;
+#pragma unroll
+        for (int d = 1; d <= D; d++) m2 += (double)u[d] * (double)u[d];
+        return make_double2(r, ((double)u[D + 1] - 0.5 * m2 * rcp_fp64(u[0])) * (gm - 1.));
+    }
+    double ek = 0;
+#pragma unroll
+    for (int d = 1; d <= D; d++) {
+        const double v = (double)u[d] / r;
+        ek += v * (double)u[d];
+    }
+    return make_double2(r, ((double)u[D + 1] - 0.5 * ek) * (gm - 1.));
 }
 
 // ---------------------------------------------------------------------------
@@ -319,23 +353,23 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // interior flux point of direction d: interpolation, primitives, Euler flux
-template <int D, int P, int TX, int TY, int TZ, int d>
-__device__ __forceinline__ void picard_interior_item(const DevGrid& G, const DevMats& M, const double* Ss,
-                                                     double* FX, int q) {
+template <typename R, int D, int P, int TX, int TY, int TZ, int d>
+__device__ __forceinline__ void picard_interior_item(const DevGrid& G, const DevMatsT<R>& M, const R* Ss,
+                                                     R* FX, int q) {
     using S = Shape<D, P>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
     constexpr int NE = TX * TY * TZ;
-    constexpr int SS = PicardPad<D, P>::SS, FXS = PicardPad<D, P>::FXS;
+    constexpr int SS = PicardPad<D, P, R>::SS, FXS = PicardPad<D, P, R>::FXS;
     const int el = q / ((nf - 2) * NTP);
     const int rr = q % ((nf - 2) * NTP);
     const int ll = 1 + rr / NTP, tp = rr % NTP;
     int c[3] = {0, 0, 0};
     tp_coords<D, n>(d, tp, c);
-    double u[V], w[V], f[V];
-    const double* src = Ss + el * SS;
+    R u[V], w[V], f[V];
+    const R* src = Ss + el * SS;
 #pragma unroll
     for (int v = 0; v < V; v++) {
-        double a = 0;
+        R a = 0;
 #pragma unroll
         for (int l = 0; l < n; l++) {
             c[d] = l;
@@ -343,11 +377,11 @@ __device__ __forceinline__ void picard_interior_item(const DevGrid& G, const Dev
         }
         u[v] = a;
     }
-    primitives<D>(u, w, G.gm);
+    primitives<D>(u, w, (R)G.gm);
     euler_flux<D>(u, w, f, d);
     c[d] = ll;
     const int fi = fp_index<n, nf>(d, c);
-    double* dst = FX + (d * NE + el) * V * FXS;
+    R* dst = FX + (d * NE + el) * V * FXS;
 #pragma unroll
     for (int v = 0; v < V; v++) dst[v * FXS + fi] = f[v];
 }
@@ -355,14 +389,14 @@ __device__ __forceinline__ void picard_interior_item(const DevGrid& G, const Dev
 // element interface of direction d: both interface states, ghost image at a
 // non-periodic domain edge (src/boundary.cpp:48-113), LLF flux written to
 // the adjacent flux points of the tile's elements
-template <int D, int P, int TX, int TY, int TZ, int d>
-__device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats& M, const double* Ss, double* FX,
+template <typename R, int D, int P, int TX, int TY, int TZ, int d>
+__device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMatsT<R>& M, const R* Ss, R* FX,
                                                  const int o[3], int q) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
     constexpr int NE = TL::NE;
-    constexpr int SS = PicardPad<D, P>::SS, FXS = PicardPad<D, P>::FXS;
+    constexpr int SS = PicardPad<D, P, R>::SS, FXS = PicardPad<D, P, R>::FXS;
     constexpr int Td = d == 0 ? TX : (d == 1 ? TY : TZ);
     constexpr int per = (NE / Td) * NTP;
     const int fidx = q / per;
@@ -380,12 +414,12 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
     const int gface = o[d] + fidx;
     const bool ghostL = gface == 0 && G.bc[d] != kPeriodic;
     const bool ghostR = gface == G.N[d] && G.bc[d] != kPeriodic;
-    double uL[V], uR[V];
+    R uL[V], uR[V];
     if (!ghostL) {
-        const double* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * SS;
+        const R* src = Ss + TL::slot(lL[0], lL[1], lL[2]) * SS;
 #pragma unroll
         for (int v = 0; v < V; v++) {
-            double a = 0;
+            R a = 0;
 #pragma unroll
             for (int l = 0; l < n; l++) {
                 c[d] = l;
@@ -395,10 +429,10 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
         }
     }
     if (!ghostR) {
-        const double* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * SS;
+        const R* src = Ss + TL::slot(lR[0], lR[1], lR[2]) * SS;
 #pragma unroll
         for (int v = 0; v < V; v++) {
-            double a = 0;
+            R a = 0;
 #pragma unroll
             for (int l = 0; l < n; l++) {
                 c[d] = l;
@@ -417,31 +451,37 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
         for (int v = 0; v < V; v++) uR[v] = uL[v];
         if (G.bc[d] == kReflective) uR[1 + d] = -uR[1 + d];
     }
-    double F[V];
-    riemann_llf<D>(F, uL, uR, d, G.gm);
+    R F[V];
+    riemann_llf<D>(F, uL, uR, d, (R)G.gm);
     if (fidx >= 1) {
         c[d] = nf - 1;
         const int fi = fp_index<n, nf>(d, c);
-        double* dst = FX + (d * NE + TL::slot(lL[0], lL[1], lL[2])) * V * FXS;
+        R* dst = FX + (d * NE + TL::slot(lL[0], lL[1], lL[2])) * V * FXS;
 #pragma unroll
         for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
     }
     if (fidx < Td) {
         c[d] = 0;
         const int fi = fp_index<n, nf>(d, c);
-        double* dst = FX + (d * NE + TL::slot(lR[0], lR[1], lR[2])) * V * FXS;
+        R* dst = FX + (d * NE + TL::slot(lR[0], lR[1], lR[2])) * V * FXS;
 #pragma unroll
         for (int v = 0; v < V; v++) dst[v * FXS + fi] = F[v];
     }
 }
+
+// resident blocks per SM the register allocation is sized for: 2 (128
+// registers a thread); 3 (85) for the FP32 form where that does not spill
+// (2D, p <= 3: its per-point slices take half the registers of FP64)
+template <typename R, int D, int P>
+constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? 3 : 2;
 
 // ---------------------------------------------------------------------------
 // Picard pass: interpolation to flux points, Euler fluxes, LLF at element
 // interfaces, flux divergence and the ADER predictor / corrector update,
 // fused so that only U_ader crosses HBM.
 // ---------------------------------------------------------------------------
-template <int D, int P, int TX, int TY, int TZ, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats M, PicardArgs A) {
+template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
+__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
@@ -451,15 +491,16 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
 
     // padded strides: an element block of the staged state (SS) and a
     // variable row of the flux-point arrays (FXS) start on different banks
-    constexpr int SS = PicardPad<D, P>::SS;
-    constexpr int FXS = PicardPad<D, P>::FXS;
+    constexpr int SS = PicardPad<D, P, R>::SS;
+    constexpr int FXS = PicardPad<D, P, R>::FXS;
     // element-slice chunks are copied by the TMA engine when they are whole
     // 16-byte units (V*NPT even); otherwise by plain loads
-    constexpr bool kBulk = (V * NPT) % 2 == 0;
-    extern __shared__ __align__(128) double smem[];
-    double* Sbuf = smem;                     // 2 x [NS][SS >= V*NPT] (double buffer)
-    double* FX = Sbuf + 2 * NS * SS;         // [D][NE][V][FXS >= NFP]
-    double* TT = FX + D * NE * V * FXS;      // [NE][V][NFP] face-integral scratch (3D)
+    constexpr bool kBulk = (V * NPT * sizeof(R)) % 16 == 0;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    R* smem = reinterpret_cast<R*>(smem_raw);
+    R* Sbuf = smem;                     // 2 x [NS][SS >= V*NPT] (R buffer)
+    R* FX = Sbuf + 2 * NS * SS;         // [D][NE][V][FXS >= NFP]
+    R* TT = FX + D * NE * V * FXS;      // [NE][V][NFP] face-integral scratch (3D)
     __shared__ long long sl_elem[NS];
     __shared__ uint64_t bar[2];
 
@@ -484,11 +525,11 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
         mbar_init(&bar[1], 1);
         mbar_fence_init();
     }
-    const double dt = *A.dt;
+    const R dt = (R)(*A.dt);
     const int nt = G.nt;
     const long long E = G.E;
 
-    double dreg[PPT][V][NT];   // kPredict: dudt per slice; kCorrect: du in [..][..][0]
+    R dreg[PPT][V][NT];   // kPredict: dudt per slice; kCorrect: du in [..][..][0]
 #pragma unroll
     for (int r = 0; r < PPT; r++)
 #pragma unroll
@@ -499,18 +540,18 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
     __syncthreads();
     // one elected thread issues the bulk copies of slice t into buffer b
     auto issue = [&](int t, int b) {
-        const double* src = A.in_slices > 1 ? A.ua_in + (long long)t * E * V * NPT : A.ua_in;
-        double* dst = Sbuf + b * NS * SS;
+        const R* src = A.in_slices > 1 ? A.ua_in + (long long)t * E * V * NPT : A.ua_in;
+        R* dst = Sbuf + b * NS * SS;
         if (kBulk) {
             if (tid == 0) {
                 uint32_t bytes = 0;
                 for (int s = 0; s < NS; s++)
-                    if (sl_elem[s] >= 0) bytes += V * NPT * sizeof(double);
+                    if (sl_elem[s] >= 0) bytes += V * NPT * sizeof(R);
                 fence_proxy_async_smem();
                 mbar_expect_tx(&bar[b], bytes);
                 for (int s = 0; s < NS; s++)
                     if (sl_elem[s] >= 0)
-                        bulk_g2s(dst + s * SS, src + sl_elem[s] * V * NPT, V * NPT * sizeof(double), &bar[b]);
+                        bulk_g2s(dst + s * SS, src + sl_elem[s] * V * NPT, V * NPT * sizeof(R), &bar[b]);
             }
         } else {
             for (int q = tid; q < NS * V * NPT; q += kThreads) {
@@ -525,7 +566,7 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
     for (int t = 0; t < nt; t++) {
         // ---- stage slice t (prefetch t+1 into the other buffer) ----
         const int b = multi ? (t & 1) : 0;
-        double* Ss = Sbuf + b * NS * SS;
+        R* Ss = Sbuf + b * NS * SS;
         if (multi && t + 1 < nt) issue(t + 1, b ^ 1);
         if (t == 0 || multi) {
             if (kBulk) mbar_wait_bounded(&bar[b], multi ? ((t >> 1) & 1) : 0, G.status);
@@ -543,14 +584,14 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
             constexpr int NFT = NF0 + NF1 + NF2;
             constexpr int total = NFT + D * NINT;
             for (int q = tid; q < total; q += kThreads) {
-                if (q < NF0) picard_face_item<D, P, TX, TY, TZ, 0>(G, M, Ss, FX, o, q);
-                else if (q < NF0 + NF1) picard_face_item<D, P, TX, TY, TZ, 1>(G, M, Ss, FX, o, q - NF0);
-                else if (D == 3 && q < NFT) picard_face_item<D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
+                if (q < NF0) picard_face_item<R, D, P, TX, TY, TZ, 0>(G, M, Ss, FX, o, q);
+                else if (q < NF0 + NF1) picard_face_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, o, q - NF0);
+                else if (D == 3 && q < NFT) picard_face_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
                 else {
                     const int r = q - NFT;
-                    if (r < NINT) picard_interior_item<D, P, TX, TY, TZ, 0>(G, M, Ss, FX, r);
-                    else if (r < 2 * NINT) picard_interior_item<D, P, TX, TY, TZ, 1>(G, M, Ss, FX, r - NINT);
-                    else picard_interior_item<D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, r - 2 * NINT);
+                    if (r < NINT) picard_interior_item<R, D, P, TX, TY, TZ, 0>(G, M, Ss, FX, r);
+                    else if (r < 2 * NINT) picard_interior_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, r - NINT);
+                    else picard_interior_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, r - 2 * NINT);
                 }
             }
         }
@@ -576,7 +617,7 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                     }
 #pragma unroll
                     for (int v = 0; v < V; v++) {
-                        double dudt = 0;
+                        R dudt = 0;
                         if (G.uniform_pow2) {
                             // every active h is the same power of two: the
                             // scaling of each term by 1/h is exact and
@@ -586,14 +627,14 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
 #pragma unroll
                                 for (int d = 0; d < D; d++)
                                     dudt += FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]] * M.dfp_to_sp[c[d] * nf + ll];
-                            dudt *= G.rh[0];
+                            dudt *= (R)G.rh[0];
                         } else {
 #pragma unroll
                             for (int ll = 0; ll < nf; ll++) {
 #pragma unroll
                                 for (int d = 0; d < D; d++) {
-                                    const double Fv = FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]];
-                                    dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], G.h[d], G.rh[d], G.pow2[d] != 0);
+                                    const R Fv = FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]];
+                                    dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], (R)G.h[d], (R)G.rh[d], G.pow2[d] != 0);
                                 }
                             }
                         }
@@ -603,12 +644,12 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                                 if (tt == t) dreg[r][v][tt] = dudt;
                         } else {
                             if (G.grav && v != 0) {
-                                const double* uv = Ss + el * SS;
-                                double s;
-                                if (v <= D) s = uv[pt] * G.g[v - 1];
+                                const R* uv = Ss + el * SS;
+                                R s;
+                                if (v <= D) s = uv[pt] * (R)G.g[v - 1];
                                 else {
-                                    s = uv[NPT + pt] * G.g[0] + uv[2 * NPT + pt] * G.g[1];
-                                    if (D == 3) s = s + uv[3 * NPT + pt] * G.g[2];
+                                    s = uv[NPT + pt] * (R)G.g[0] + uv[2 * NPT + pt] * (R)G.g[1];
+                                    if (D == 3) s = s + uv[3 * NPT + pt] * (R)G.g[2];
                                 }
                                 dudt -= s;
                             }
@@ -619,11 +660,11 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
             }
         } else {
             // ---- FV face fluxes of slice t (src/transforms.cpp:378-481) ----
-            const double* Mc = M.sp_to_cv;
+            const R* Mc = M.sp_to_cv;
 #pragma unroll
             for (int d = 0; d < D; d++) {
-                double* out = A.ff[d];
-                const double* Fd = FX + d * NE * V * FXS;
+                R* out = A.ff[d];
+                const R* Fd = FX + d * NE * V * FXS;
                 if (D == 2) {
                     for (int q = tid; q < NE * NFP; q += kThreads) {
                         const int el = q / NFP, fi = q % NFP;
@@ -631,11 +672,11 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                         int ll, cc;
                         if (d == 0) { ll = fi % nf; cc = fi / nf; }
                         else { cc = fi % n; ll = fi / n; }
-                        double* dst = out + (((long long)t * E + sl_elem[el]) * V) * NFP + fi;
-                        const double* srcb = Fd + el * V * FXS + (d == 0 ? ll : n * ll);
+                        R* dst = out + (((long long)t * E + sl_elem[el]) * V) * NFP + fi;
+                        const R* srcb = Fd + el * V * FXS + (d == 0 ? ll : n * ll);
 #pragma unroll
                         for (int v = 0; v < V; v++) {
-                            double f = 0;
+                            R f = 0;
 #pragma unroll
                             for (int m = 0; m < n; m++)
                                 f += srcb[v * FXS + (d == 0 ? nf * m : m)] * Mc[cc * n + m];
@@ -655,7 +696,7 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                         else if (d == 1) { c[0] = fi % n; c[1] = (fi / n) % nf; c[2] = fi / (n * nf); }
                         else { c[0] = fi % n; c[1] = (fi / n) % n; c[2] = fi / (n * n); }
                         const int id = c[d1];
-                        double u = 0;
+                        R u = 0;
 #pragma unroll
                         for (int m = 0; m < n; m++) {
                             c[d1] = m;
@@ -673,7 +714,7 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                         else if (d == 1) { c[0] = fi % n; c[1] = (fi / n) % nf; c[2] = fi / (n * nf); }
                         else { c[0] = fi % n; c[1] = (fi / n) % n; c[2] = fi / (n * n); }
                         const int id = c[d2];
-                        double f = 0;
+                        R f = 0;
 #pragma unroll
                         for (int m = 0; m < n; m++) {
                             c[d2] = m;
@@ -696,20 +737,20 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
             if (q < NE * NPT) {
                 const int el = q / NPT, pt = q % NPT;
                 const long long ge = sl_elem[el];
-                double nw[D + 1][NT];  // updated rho and momenta (gravity of later slots)
+                R nw[D + 1][NT];  // updated rho and momenta (gravity of later slots)
 #pragma unroll
                 for (int v = 0; v < V; v++) {
-                    const double u_old = A.u[(ge * V + v) * NPT + pt];
-                    double dudt[NT];
+                    const R u_old = A.u[(ge * V + v) * NPT + pt];
+                    R dudt[NT];
 #pragma unroll
                     for (int tt = 0; tt < NT; tt++) {
                         dudt[tt] = dreg[r][v][tt];
                         if (G.grav && v != 0 && tt < nt) {
-                            double s;
-                            if (v <= D) s = nw[0][tt] * G.g[v - 1];
+                            R s;
+                            if (v <= D) s = nw[0][tt] * (R)G.g[v - 1];
                             else {
-                                s = nw[1][tt] * G.g[0] + nw[2][tt] * G.g[1];
-                                if (D == 3) s = s + nw[3][tt] * G.g[2];
+                                s = nw[1][tt] * (R)G.g[0] + nw[2][tt] * (R)G.g[1];
+                                if (D == 3) s = s + nw[3][tt] * (R)G.g[2];
                             }
                             dudt[tt] -= s;
                         }
@@ -717,11 +758,11 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
 #pragma unroll
                     for (int tt = 0; tt < NT; tt++) {
                         if (tt >= nt) break;
-                        double du = 0;
+                        R du = 0;
 #pragma unroll
                         for (int ll = 0; ll < NT; ll++)
                             if (ll < nt) du += dudt[ll] * M.invader[tt * nt + ll] * M.wt[ll] * dt;
-                        const double val = u_old - du;
+                        const R val = u_old - du;
                         if (v <= D) nw[v][tt] = val;
                         A.ua_out[(((long long)tt * E + ge) * V + v) * NPT + pt] = val;
                     }
@@ -730,26 +771,29 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
         }
     } else if (MODE == kCorrect) {
         // ---- corrector / RK stage (src/transforms.cpp:327-374, 252-261) ----
-        double* Wsp = Sbuf;                // reuse staging memory: [NE][V][NPT]
-        double* Tmp = Sbuf + NE * V * NPT;
+        R* Wsp = Sbuf;                // reuse staging memory: [NE][V][NPT]
+        R* Tmp = Sbuf + NE * V * NPT;
 #pragma unroll
         for (int r = 0; r < PPT; r++) {
             const int q = tid + r * kThreads;
             if (q < NE * NPT) {
                 const int el = q / NPT, pt = q % NPT;
                 const long long ge = sl_elem[el];
-                double un[V];
+                R un[V];
 #pragma unroll
                 for (int v = 0; v < V; v++) {
                     const long long gi = (ge * V + v) * NPT + pt;
-                    double val = A.u[gi] - dreg[r][v][0];
-                    if (A.rk_a > 0) val = A.rk_a * A.u0[gi] + (1.0 - A.rk_a) * val;
+                    R val = A.u[gi] - dreg[r][v][0];
+                    if (A.rk_a > 0) {
+                        const R ra = (R)A.rk_a;
+                        val = ra * A.u0[gi] + ((R)1.0 - ra) * val;
+                    }
                     un[v] = val;
                     A.u_out[gi] = val;
                 }
                 if (A.final_stage) {
-                    double w[V];
-                    primitives<D>(un, w, G.gm);
+                    R w[V];
+                    primitives<D>(un, w, (R)G.gm);
 #pragma unroll
                     for (int v = 0; v < V; v++) Wsp[(el * V + v) * NPT + pt] = w[v];
                 }
@@ -758,11 +802,11 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
         if (A.final_stage) {
             __syncthreads();
             // W_cv = sp_to_cv(W_sp): x, y(, z) sweeps (src/transforms.cpp:99-117)
-            double* bufs[2] = {Tmp, Wsp};
-            const double* src = Wsp;
+            R* bufs[2] = {Tmp, Wsp};
+            const R* src = Wsp;
             for (int d = 0; d < D; d++) {
-                double* dst = bufs[d % 2];
-                sweep_smem<D, P>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+                R* dst = bufs[d % 2];
+                sweep_smem<D, P, R>(src, dst, M.sp_to_cv, d, NE * V * NPT);
                 __syncthreads();
                 src = dst;
             }
@@ -773,7 +817,7 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
                 if (q < NE * NPT) {
                     const int el = q / NPT, pt = q % NPT;
                     const long long ge = sl_elem[el];
-                    double w[V];
+                    R w[V];
 #pragma unroll
                     for (int v = 0; v < V; v++) w[v] = src[(el * V + v) * NPT + pt];
                     if (A.wcv)
@@ -786,18 +830,18 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
         }
     } else {
         // ---- U_cv = sp_to_cv(U) and the slice-0 FV candidate ----
-        double* Ut = Sbuf;
-        double* Tmp = Sbuf + NE * V * NPT;
+        R* Ut = Sbuf;
+        R* Tmp = Sbuf + NE * V * NPT;
         for (int q = tid; q < NE * V * NPT; q += kThreads) {
             const int el = q / (V * NPT), off = q % (V * NPT);
             Ut[q] = A.u[sl_elem[el] * V * NPT + off];
         }
         __syncthreads();
-        double* bufs[2] = {Tmp, Ut};
-        const double* src = Ut;
+        R* bufs[2] = {Tmp, Ut};
+        const R* src = Ut;
         for (int d = 0; d < D; d++) {
-            double* dst = bufs[d % 2];
-            sweep_smem<D, P>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+            R* dst = bufs[d % 2];
+            sweep_smem<D, P, R>(src, dst, M.sp_to_cv, d, NE * V * NPT);
             __syncthreads();
             src = dst;
         }
@@ -808,29 +852,27 @@ __global__ void __launch_bounds__(kThreads, 2) picard_kernel(DevGrid G, DevMats 
         for (int q = tid; q < NE * NPT; q += kThreads) {
             const int el = q / NPT, pt = q % NPT;
             const long long ge = sl_elem[el];
-            double uo[V], un[V], w[V];
+            R uo[V], un[V];
 #pragma unroll
             for (int v = 0; v < V; v++) uo[v] = src[(el * V + v) * NPT + pt];
-            fv_candidate<D, P>(G, A.ff, 0, ge, pt, uo, M.wt[0] * dt, un);
-            primitives<D>(uo, w, G.gm);
-            A.rp_old[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
-            primitives<D>(un, w, G.gm);
-            A.rp_new[ge * NPT + pt] = make_double2(w[0], w[D + 1]);
+            fv_candidate<D, P, R>(G, A.ff, 0, ge, pt, uo, M.wt[0] * dt, un);
+            A.rp_old[ge * NPT + pt] = rho_p_fp64<D>(uo, G.gm);
+            A.rp_new[ge * NPT + pt] = rho_p_fp64<D>(un, G.gm);
         }
     }
 }
 
-template <int D, int P, int TX, int TY, int TZ>
+template <typename R, int D, int P, int TX, int TY, int TZ>
 constexpr size_t picard_smem_bytes() {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
-    size_t a = 2 * (size_t)TL::NS * PicardPad<D, P>::SS;
-    size_t b = (size_t)D * TL::NE * S::V * PicardPad<D, P>::FXS;
+    size_t a = 2 * (size_t)TL::NS * PicardPad<D, P, R>::SS;
+    size_t b = (size_t)D * TL::NE * S::V * PicardPad<D, P, R>::FXS;
     size_t c = (size_t)TL::NE * S::V * S::NFP;
     size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
     size_t total = a + b + c;
     if (need_epi > total) total = need_epi;
-    return total * sizeof(double);
+    return total * sizeof(R);
 }
 
 }  // namespace spdk

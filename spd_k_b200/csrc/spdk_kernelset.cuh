@@ -14,65 +14,65 @@ namespace spdk {
 // ---------------------------------------------------------------------------
 // U_sp = conservatives(cv_to_sp(W_cv)) and dt(W_cv): the constructor tail
 // (src/hydro_ader.hpp:205-208)
-template <int D, int P>
-__global__ void __launch_bounds__(kThreads) init_state_kernel(DevGrid G, DevMats M, const double* __restrict__ wcv,
-                                                             double* __restrict__ u,
+template <typename R, int D, int P>
+__global__ void __launch_bounds__(kThreads) init_state_kernel(DevGrid G, DevMatsT<R> M, const R* __restrict__ wcv,
+                                                             R* __restrict__ u,
                                                              unsigned long long* dtmin) {
     using S = Shape<D, P>;
     constexpr int V = S::V, NPT = S::NPT;
-    __shared__ double b0[V * NPT], b1[V * NPT];
+    __shared__ R b0[V * NPT], b1[V * NPT];
     const long long ge = blockIdx.x;
     for (int q = threadIdx.x; q < V * NPT; q += blockDim.x) b0[q] = wcv[ge * V * NPT + q];
     __syncthreads();
     double dtl = 1.7976931348623157e308;
     for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V];
+        R w[V];
         for (int v = 0; v < V; v++) w[v] = b0[v * NPT + q];
         dtl = smin(dtl, point_dt<D>(G, w, S::n));
     }
-    double* bufs[2] = {b1, b0};
-    const double* src = b0;
+    R* bufs[2] = {b1, b0};
+    const R* src = b0;
     for (int d = 0; d < D; d++) {
-        double* dst = bufs[d % 2];
-        sweep_smem<D, P>(src, dst, M.cv_to_sp, d, V * NPT);
+        R* dst = bufs[d % 2];
+        sweep_smem<D, P, R>(src, dst, M.cv_to_sp, d, V * NPT);
         __syncthreads();
         src = dst;
     }
     for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V], uu[V];
+        R w[V], uu[V];
         for (int v = 0; v < V; v++) w[v] = src[v * NPT + q];
-        conservatives<D>(w, uu, G.gm);
+        conservatives<D>(w, uu, (R)G.gm);
         for (int v = 0; v < V; v++) u[ge * V * NPT + v * NPT + q] = uu[v];
     }
     block_min_dt(dtl, dtmin);
 }
 
 // W_cv = sp_to_cv(primitives(U_sp)) and dt, for a state written by the host
-template <int D, int P>
-__global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMats M, const double* __restrict__ u,
-                                                         double* __restrict__ wcv, unsigned long long* dtmin) {
+template <typename R, int D, int P>
+__global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMatsT<R> M, const R* __restrict__ u,
+                                                         R* __restrict__ wcv, unsigned long long* dtmin) {
     using S = Shape<D, P>;
     constexpr int V = S::V, NPT = S::NPT;
-    __shared__ double b0[V * NPT], b1[V * NPT];
+    __shared__ R b0[V * NPT], b1[V * NPT];
     const long long ge = blockIdx.x;
     for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double uu[V], w[V];
+        R uu[V], w[V];
         for (int v = 0; v < V; v++) uu[v] = u[ge * V * NPT + v * NPT + q];
-        primitives<D>(uu, w, G.gm);
+        primitives<D>(uu, w, (R)G.gm);
         for (int v = 0; v < V; v++) b0[v * NPT + q] = w[v];
     }
     __syncthreads();
-    double* bufs[2] = {b1, b0};
-    const double* src = b0;
+    R* bufs[2] = {b1, b0};
+    const R* src = b0;
     for (int d = 0; d < D; d++) {
-        double* dst = bufs[d % 2];
-        sweep_smem<D, P>(src, dst, M.sp_to_cv, d, V * NPT);
+        R* dst = bufs[d % 2];
+        sweep_smem<D, P, R>(src, dst, M.sp_to_cv, d, V * NPT);
         __syncthreads();
         src = dst;
     }
     double dtl = 1.7976931348623157e308;
     for (int q = threadIdx.x; q < NPT; q += blockDim.x) {
-        double w[V];
+        R w[V];
         for (int v = 0; v < V; v++) {
             w[v] = src[v * NPT + q];
             wcv[ge * V * NPT + v * NPT + q] = w[v];
@@ -89,34 +89,36 @@ static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin) 
 }
 
 // ---------------------------------------------------------------------------
-// kernel table of one (D, P, tile) instantiation
+// kernel table of one (R, D, P, tile) instantiation
 // ---------------------------------------------------------------------------
-struct KernelSet {
-    void (*predict)(DevGrid, DevMats, PicardArgs) = nullptr;
-    void (*correct)(DevGrid, DevMats, PicardArgs) = nullptr;
-    void (*flux)(DevGrid, DevMats, PicardArgs) = nullptr;
+template <typename R>
+struct KernelSetT {
+    void (*predict)(DevGrid, DevMatsT<R>, PicardArgsT<R>) = nullptr;
+    void (*correct)(DevGrid, DevMatsT<R>, PicardArgsT<R>) = nullptr;
+    void (*flux)(DevGrid, DevMatsT<R>, PicardArgsT<R>) = nullptr;
     void (*detect)(DevGrid, const double2*, const double2*, uint8_t*, int*) = nullptr;
     void (*theta)(DevGrid, const uint8_t*, uint8_t*) = nullptr;
-    void (*update)(DevGrid, DevMats, FallbackArgs) = nullptr;
-    void (*init)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
-    void (*derive)(DevGrid, DevMats, const double*, double*, unsigned long long*) = nullptr;
+    void (*update)(DevGrid, DevMatsT<R>, FallbackArgsT<R>) = nullptr;
+    void (*init)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
+    void (*derive)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
     size_t picard_smem = 0, update_smem = 0;
     int tile[3] = {1, 1, 1};
 };
+using KernelSet = KernelSetT<double>;
 
-template <int D, int P, int TX, int TY, int TZ>
-KernelSet make_set() {
-    KernelSet k;
-    k.predict = picard_kernel<D, P, TX, TY, TZ, kPredict>;
-    k.correct = picard_kernel<D, P, TX, TY, TZ, kCorrect>;
-    k.flux = picard_kernel<D, P, TX, TY, TZ, kFlux>;
-    k.detect = fv_detect_kernel<D, P, TX, TY, TZ>;
-    k.theta = fv_theta_kernel<D, P, TX, TY, TZ>;
-    k.update = fv_update_kernel<D, P, TX, TY, TZ>;
-    k.init = init_state_kernel<D, P>;
-    k.derive = derive_kernel<D, P>;
-    k.picard_smem = picard_smem_bytes<D, P, TX, TY, TZ>();
-    k.update_smem = UpdateSmem<D, P, TX, TY, TZ>::bytes;
+template <typename R, int D, int P, int TX, int TY, int TZ>
+KernelSetT<R> make_set() {
+    KernelSetT<R> k;
+    k.predict = picard_kernel<R, D, P, TX, TY, TZ, kPredict>;
+    k.correct = picard_kernel<R, D, P, TX, TY, TZ, kCorrect>;
+    k.flux = picard_kernel<R, D, P, TX, TY, TZ, kFlux>;
+    k.detect = fv_detect_kernel<R, D, P, TX, TY, TZ>;
+    k.theta = fv_theta_kernel<R, D, P, TX, TY, TZ>;
+    k.update = fv_update_kernel<R, D, P, TX, TY, TZ>;
+    k.init = init_state_kernel<R, D, P>;
+    k.derive = derive_kernel<R, D, P>;
+    k.picard_smem = picard_smem_bytes<R, D, P, TX, TY, TZ>();
+    k.update_smem = UpdateSmem<R, D, P, TX, TY, TZ>::bytes;
     k.tile[0] = TX;
     k.tile[1] = TY;
     k.tile[2] = TZ;
@@ -124,29 +126,37 @@ KernelSet make_set() {
 }
 
 // Tile choice: the largest instantiated tile that divides the element counts.
-template <int P>
-bool pick2(int Nx, int Ny, KernelSet* k) {
+template <typename R, int P>
+bool pick2(int Nx, int Ny, KernelSetT<R>* k) {
     if constexpr (P <= 4) {
-        if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<2, P, 4, 4, 1>(); return true; }
+        if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<R, 2, P, 4, 4, 1>(); return true; }
     }
-    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<2, P, 2, 2, 1>(); return true; }
-    *k = make_set<2, P, 1, 1, 1>();
+    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<R, 2, P, 2, 2, 1>(); return true; }
+    *k = make_set<R, 2, P, 1, 1, 1>();
     return true;
 }
-template <int P>
-bool pick3(int, int, int, KernelSet* k) {
-    *k = make_set<3, P, 1, 1, 1>();
+template <typename R, int P>
+bool pick3(int, int, int, KernelSetT<R>* k) {
+    *k = make_set<R, 3, P, 1, 1, 1>();
     return true;
 }
 
-// per-translation-unit selectors (spdk_select_*.cu)
-bool select_2d_low(int p, const int N[3], KernelSet* k);   // p = 1..3
-bool select_2d_high(int p, const int N[3], KernelSet* k);  // p = 4..7
-bool select_3d(int p, const int N[3], KernelSet* k);       // p = 1..5
+// per-translation-unit selectors (spdk_select_*.cu): the FP64 units are
+// compiled without FMA contraction (reference rounding), the FP32 units with it
+bool select_2d_low(int p, const int N[3], KernelSetT<double>* k);   // p = 1..3
+bool select_2d_high(int p, const int N[3], KernelSetT<double>* k);  // p = 4..7
+bool select_3d(int p, const int N[3], KernelSetT<double>* k);       // p = 1..5
+bool select_f32_2d(int p, const int N[3], KernelSetT<float>* k);    // p = 1..7
+bool select_f32_3d(int p, const int N[3], KernelSetT<float>* k);    // p = 1..5
 
-inline bool select_kernels(int D, int p, const int N[3], KernelSet* k) {
+inline bool select_kernels(int D, int p, const int N[3], KernelSetT<double>* k) {
     if (D == 2) return p <= 3 ? select_2d_low(p, N, k) : select_2d_high(p, N, k);
     if (D == 3) return select_3d(p, N, k);
+    return false;
+}
+inline bool select_kernels(int D, int p, const int N[3], KernelSetT<float>* k) {
+    if (D == 2) return select_f32_2d(p, N, k);
+    if (D == 3) return select_f32_3d(p, N, k);
     return false;
 }
 

@@ -1,9 +1,10 @@
 // Pointwise Euler physics shared by the spd_K B200 kernels.
 //
 // Every routine evaluates the same floating-point operations in the same
-// order as the reference routine cited beside it. The parity build compiles
-// with -fmad=false, so no product is fused into a sum and FP64 results are
-// bit-identical to the reference's x86-64 CPU build. Conserved slots are
+// order as the reference routine cited beside it. For R = double (the plain
+// form) the build compiles with -fmad=false, so no product is fused into a
+// sum and FP64 results are bit-identical to the reference's x86-64 CPU build;
+// R = float is the precision form (FMA allowed, FP64 islands where noted). Conserved slots are
 // rho, m_1..m_D, E (V = D+2): in 2D the reference also carries m_z = 0,
 // whose terms only ever add or multiply signed zeros, so they are dropped.
 #pragma once
@@ -28,16 +29,42 @@ template <typename R> __device__ __forceinline__ R sound_speed(R rho, R p, R gm)
     return sqrt(c2);
 }
 
-// src/hydro.cpp:95-106: w = (rho, v_1..v_D, p)
+// 1/x in FP64 for an FP32 x: an FP32 seed refined by two Newton-Raphson
+// steps r <- r + r(1 - x r) (each squares the relative error: 1e-7 -> 1e-14
+// -> below FP64 rounding), without a double-precision division
+__device__ __forceinline__ double rcp_fp64(float x) {
+    const double xd = x;
+    double r = (double)(1.0f / x);
+    r = r + r * (1.0 - xd * r);
+    r = r + r * (1.0 - xd * r);
+    return r;
+}
+
+// src/hydro.cpp:95-106: w = (rho, v_1..v_D, p). In the FP32 precision form
+// the pressure is recovered in FP64: E - |m|^2/(2 rho) cancels badly where
+// the kinetic energy nearly equals the total energy, so |m|^2 is formed from
+// exact FP64 products of the FP32 momenta and divided by rho in FP64.
 template <int D, typename R> __device__ __forceinline__ void primitives(const R* u, R* w, R gm) {
-    R ek = 0;
-    w[0] = u[0];
+    if constexpr (sizeof(R) == 4) {
+        const float rf = 1.0f / u[0];
+        double m2 = 0;
+        w[0] = u[0];
 #pragma unroll
-    for (int d = 1; d <= D; d++) {
-        w[d] = u[d] / u[0];
-        ek += w[d] * u[d];
+        for (int d = 1; d <= D; d++) {
+            w[d] = u[d] * rf;
+            m2 += (double)u[d] * (double)u[d];
+        }
+        w[D + 1] = (R)(((double)u[D + 1] - 0.5 * m2 * rcp_fp64(u[0])) * ((double)gm - 1.0));
+    } else {
+        R ek = 0;
+        w[0] = u[0];
+#pragma unroll
+        for (int d = 1; d <= D; d++) {
+            w[d] = u[d] / u[0];
+            ek += w[d] * u[d];
+        }
+        w[D + 1] = (u[D + 1] - R(0.5) * ek) * (gm - R(1.));
     }
-    w[D + 1] = (u[D + 1] - R(0.5) * ek) * (gm - R(1.));
 }
 
 // src/hydro.cpp:34-45

@@ -1,0 +1,234 @@
+"""The FP32 precision form against the plain FP64 form on the same GPU.
+
+The precision form keeps the state, the transforms and the fluxes in FP32
+(FMA contraction allowed) and computes in FP64 the pressure recovery
+p = (E - m.v/2)(gamma-1), the (rho, p) candidates that the NAD/SED/PAD
+detector compares against their bounds, and the dt reduction. It makes no
+bitwise claim; each test states its relative-L1 tolerance per field,
+sum|a - b| / sum|b| over the active sub-cells, b the FP64 result.
+"""
+import zlib
+
+import numpy as np
+import pytest
+
+from helpers import gpu_config
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("rho", "m1", "m2", "m3", "E")
+
+
+def solver(overrides, precision, **extra):
+    import spd_k_b200 as S
+    return S.HydroSolver(dict(gpu_config(overrides), precision=precision, **extra))
+
+
+def rel_l1_per_field(a, b):
+    """a, b: (V, ...) arrays -> relative L1 of each var; a field that is zero
+    up to round-off in b (z momentum of a flow in the x-y plane) is measured
+    against the L1 norm of the density instead"""
+    n0 = np.abs(b[0]).sum()
+    out = []
+    for v in range(b.shape[0]):
+        nv = np.abs(b[v]).sum()
+        out.append(float(np.abs(a[v] - b[v]).sum() / (nv if nv > 1e-6 * n0 else n0)))
+    return out
+
+
+def report(name, errs, V):
+    names = FIELDS[:V - 1] + ("E",) if V == 4 else FIELDS
+    print(f"\n{name}: " + ", ".join(f"{k}={e:.3e}" for k, e in zip(names, errs)))
+
+
+def random_u(g, seed):
+    rng = np.random.default_rng(seed)
+    E, V, npt = g.info.n_elements, g.info.nvar, g.info.n_points
+    D = g.info.ndim
+    rho = rng.uniform(0.5, 1.5, (E, npt))
+    vel = [rng.uniform(-0.5, 0.5, (E, npt)) for _ in range(D)]
+    p = rng.uniform(0.5, 1.5, (E, npt))
+    gm = g.c["gamma"]
+    ek = sum(v * rho * v for v in vel)
+    en = p / (gm - 1.0) + 0.5 * ek
+    return np.stack([rho] + [rho * v for v in vel] + [en], axis=1)
+
+
+SMOOTH_CASES = {
+    # smooth sine-wave advection without the limiter. (A random state without
+    # the limiter is no usable comparison: it blows up within three steps and
+    # a 1e-7 relative perturbation of it changes the result by O(1) in FP64
+    # alone. At p >= 5 the scheme itself is unstable at CFL 0.8 -- the oracle
+    # blows up within 20-30 steps in FP64 -- so those cases run at CFL 0.4.)
+    "2d_p3_ader": ["job/fallback=false", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1"],
+    "2d_p4_ader": ["job/fallback=false", "mesh/p=4", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=1"],
+    "2d_p5_rk3": ["job/fallback=false", "mesh/p=5", "mesh/nx1=4", "mesh/nx2=6", "mesh/nx3=1",
+                  "time/integrator=rk3", "time/cfl=0.4"],
+    "2d_p7_ader": ["job/fallback=false", "mesh/p=7", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=1", "time/cfl=0.4"],
+    "3d_p3_ader_gravity": ["job/fallback=false", "mesh/nx1=3", "mesh/nx2=4", "mesh/nx3=2", "hydro/g3=0.3"],
+    "3d_p5_ader": ["job/fallback=false", "mesh/p=5", "mesh/nx1=2", "mesh/nx2=2", "mesh/nx3=2", "time/cfl=0.4"],
+    "3d_p2_rk2": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=4",
+                  "time/integrator=rk2"],
+}
+
+
+@pytest.mark.parametrize("case", sorted(SMOOTH_CASES))
+def test_smooth_steps_against_fp64(case):
+    """20 steps of smooth flow: FP32 round-off only (relative L1 of U_sp
+    below 3e-6 per conserved field -- a field growing from zero, like the
+    z momentum under z gravity, sits at the top of that range; dt within
+    1e-6 relative)."""
+    ov = SMOOTH_CASES[case]
+    g64, g32 = solver(ov, "fp64"), solver(ov, "fp32")
+    assert abs(g32.dt() - g64.dt()) <= 1e-6 * g64.dt()
+    for _ in range(20):
+        g64.step()
+        g32.step()
+    errs = rel_l1_per_field(g32.field_array(0), g64.field_array(0))
+    report(case, errs, g64.info.nvar)
+    assert max(errs) < 3e-6, errs
+    assert abs(g32.dt() - g64.dt()) <= 1e-6 * g64.dt()
+    g64.close()
+    g32.close()
+
+
+def test_fallback_step_from_random_state():
+    """A state that trips the detector everywhere: the FP64 candidates and
+    bound comparisons keep the trouble flags of the two forms (nearly)
+    identical, so the step differs by FP32 round-off plus the few sub-cells
+    whose candidate sits within round-off of its NAD bound."""
+    ov = ["job/fallback=true", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1"]
+    g64, g32 = solver(ov, "fp64"), solver(ov, "fp32")
+    u = random_u(g64, 11)
+    g64.write_u(u)
+    g32.write_u(u)
+    g64.step()
+    g32.step()
+    t64, t32 = g64.read(2), g32.read(2)
+    frac = float(np.mean(t64 != t32))
+    errs = rel_l1_per_field(g32.field_array(0), g64.field_array(0))
+    report("fallback random", errs, g64.info.nvar)
+    print(f"trouble flags differing: {frac:.4f} of {t64.size} (fp64 flags {int(t64.sum())})")
+    assert t64.sum() > 0
+    assert frac < 0.02
+    assert max(errs) < 1e-3, errs
+    g64.close()
+    g32.close()
+
+
+def test_sine_wave_config1_error_against_exact():
+    """32x32, p=3 sine wave to t=1 (725 steps). The FP64 form's L1 error
+    against the exact profile is the discretisation error (~5e-8); FP32
+    round-off over 725 steps adds to it: the precision form's error stays
+    below 1e-6 (relative L1 against FP64 < 5e-6 per field)."""
+    import spd_k_b200 as S
+    from helpers import manifest
+    ov = manifest()["full_cases"]["config1_sine2d_32"]["overrides"]
+    out = {}
+    for prec in ("fp64", "fp32"):
+        g = solver(ov, prec)
+        g.run(g.c["tlim"], g.c["output_dt"])
+        out[prec] = (g.field_array(S.FIELD_W_CV), g.n_step)
+        g.close()
+    (w64, n64), (w32, n32) = out["fp64"], out["fp32"]
+    assert n64 == 725 and abs(n32 - n64) <= 1
+    # exact solution: the initial sub-cell averages (one period of advection)
+    g0 = solver(ov, "fp64")
+    w0 = g0.field_array(S.FIELD_W_CV)
+    g0.close()
+    e64 = float(np.abs(w64[0] - w0[0]).mean())
+    e32 = float(np.abs(w32[0] - w0[0]).mean())
+    d = rel_l1_per_field(w32, w64)
+    print(f"\nsine L1(rho) vs exact: fp64 {e64:.3e}  fp32 {e32:.3e};  fp32 vs fp64 per field {d}")
+    assert e64 < 1e-7
+    assert e32 < 1e-5
+    assert d[0] < 1e-5 and d[-1] < 1e-5
+
+
+def element_means(g):
+    """exact element means of the conserved fields from U_sp: the
+    interpolating polynomial through the solution points integrated by
+    Gauss-Legendre quadrature -> (V, Ny, Nx) for a 2D run"""
+    n = g.p + 1
+    x_sp = 0.5 * (1.0 - np.cos((2 * np.arange(n) + 1) / (2.0 * n) * np.pi))
+    xq, wq = np.polynomial.legendre.leggauss(n)
+    xq, wq = (xq + 1) / 2, wq / 2
+    lag = np.array([[np.prod([(x - x_sp[k]) / (x_sp[j] - x_sp[k]) for k in range(n) if k != j]) for x in xq]
+                    for j in range(n)])
+    w1 = lag @ wq                                    # integral of each Lagrange basis over [0, 1]
+    u = g.field_array(0)[:, 0, :, :, 0]              # (V, Ny, Nx, ny, nx)
+    return np.einsum("vyxji,j,i->vyx", u, w1, w1)
+
+
+def blast_error_pair(N, t_end):
+    """L1 of the element means of (rho, m, E) against an FP64 run on the 2N
+    mesh (2x2 fine element means averaged onto each coarse element), for the
+    FP64 and the FP32 form on the N mesh, and their own difference"""
+    import bench
+    fine = solver(bench.workload_overrides(2 * N) + [f"time/tlim={t_end!r}", f"output/dt={t_end!r}"], "fp64")
+    fine.run(t_end, t_end)
+    mf = element_means(fine)
+    fine.close()
+    V = mf.shape[0]
+    mref = mf.reshape(V, N, 2, N, 2).mean(axis=(2, 4))
+    res = {}
+    for prec in ("fp64", "fp32"):
+        g = solver(bench.workload_overrides(N) + [f"time/tlim={t_end!r}", f"output/dt={t_end!r}"], prec)
+        g.run(t_end, t_end)
+        assert abs(g.t - t_end) < 1e-12
+        res[prec] = element_means(g)
+        g.close()
+    err = {k: [float(np.abs(v[i] - mref[i]).mean()) for i in range(V)] for k, v in res.items()}
+    diff = rel_l1_per_field(res["fp32"], res["fp64"])
+    return err, diff
+
+
+def test_blast_64_matched_error():
+    """The benchmark blast geometry at 64x64 to t=0.005: the shock's detector
+    decisions amplify round-off (the reference itself moves by 1e-4..8e-3
+    relative L1 after 94 steps from a one-ulp change of the initial state),
+    so the two forms are compared by their error against an FP64 run on the
+    128x128 mesh: the FP32 form's L1 error of every conserved field's element
+    means is within 1.1x of the FP64 form's."""
+    err, diff = blast_error_pair(64, 0.005)
+    print(f"\nblast 64 vs fp64 128: fp64 {err['fp64']}\n                      fp32 {err['fp32']}"
+          f"\nfp32 vs fp64 relative L1 {diff}")
+    for e64, e32 in zip(err["fp64"], err["fp32"]):
+        assert e32 <= 1.1 * e64
+
+
+def test_blast_256_mass_and_positivity():
+    """Benchmark size, 40 graph-replayed steps of the precision form: mass
+    conserved to FP32 round-off (relative 1e-6), finite, density positive."""
+    import bench
+    g = solver(bench.workload_overrides(256), "fp32")
+    n = 4
+    w0 = g.field_array(1)
+    g.steps(40)
+    g.sync()
+    w = g.field_array(1)
+    assert np.all(np.isfinite(w)) and np.all(np.isfinite(g.field_array(0)))
+    # mass: sub-cell averages of rho times sub-cell volumes (sub-cell faces at
+    # 0, the p Gauss-Legendre points and 1 of each element), summed in FP64
+    xg = (np.polynomial.legendre.leggauss(3)[0] + 1) / 2
+    hx = np.tile(np.diff(np.concatenate([[0.0], xg, [1.0]])), 256) / 256
+    vol = hx[:, None] * hx[None, :]
+    def mass(a):
+        rho = a[0, 0, :, :, 0].transpose(0, 2, 1, 3).reshape(256 * n, 256 * n)
+        return float((rho * vol).sum())
+    m0, m1 = mass(w0), mass(w)
+    print(f"\nmass drift {abs(m1 - m0) / m0:.3e}")
+    assert abs(m1 - m0) / m0 < 1e-6
+    assert float(w[0].min()) > 0
+    g.close()
+
+
+def test_blast_256_to_t005_matched_error():
+    """The full 2D point blast (256x256, p=3, to t=0.05): both forms' L1
+    errors of the element means against an FP64 run on 512x512, the FP32
+    form's within 2x of the FP64 form's on every conserved field."""
+    err, diff = blast_error_pair(256, 0.05)
+    print(f"\nblast 256 vs fp64 512: fp64 {err['fp64']}\n                       fp32 {err['fp32']}"
+          f"\nfp32 vs fp64 relative L1 {diff}")
+    for e64, e32 in zip(err["fp64"], err["fp32"]):
+        assert e32 <= 2.0 * e64
