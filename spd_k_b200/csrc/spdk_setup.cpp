@@ -295,6 +295,7 @@ void build_matrices(int p, bool ader, Matrices* m) {
         for (int i = 0; i < nf; i++) m->dfp_to_sp[j * nf + i] = lagrange_prime(m->x_fp, m->x_sp[j], i, nf);
     integral_matrix(m->sp_to_cv, m->x_fp, m->x_sp, n, n);
     inverse(m->sp_to_cv, m->cv_to_sp, n);
+    integral_matrix(m->fp_to_cv, m->x_fp, m->x_fp, n, nf);
     if (ader) {
         m->nt = n;
         for (int i = 0; i < n; i++) {
@@ -326,6 +327,7 @@ void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a
     a->fvn = N * nsp + 4;
     const int idL = nsp - 2, idR = a->fvn + idL;
     a->sd_faces.assign((size_t)Ntot * nfp, 0.0);
+    a->sd_centers.assign((size_t)Ntot * nsp, 0.0);
     a->fv_faces.assign(a->fvn + 1, 0.0);
     a->fv_centers.assign(a->fvn, 0.0);
     for (int j = 0; j < Ntot; j++) {
@@ -337,6 +339,7 @@ void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a
         }
         for (int i = 0; i < nsp; i++) {
             const double c = 0.5 * (a->sd_faces[j * nfp + i + 1] + a->sd_faces[j * nfp + i]);
+            a->sd_centers[j * nsp + i] = c;
             const int g = i + j * nsp;
             if (g >= idL && g < idR) a->fv_centers[i - idL + j * nsp] = c;
         }

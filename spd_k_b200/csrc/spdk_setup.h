@@ -24,6 +24,7 @@ struct Matrices {
     double dfp_to_sp[kMaxN * kMaxNF] = {};  // [n][nf]
     double sp_to_cv[kMaxN * kMaxN] = {};
     double cv_to_sp[kMaxN * kMaxN] = {};
+    double fp_to_cv[kMaxN * kMaxNF] = {};   // [n][nf] (src/induction_ader.hpp:149)
     double ader[kMaxN * kMaxN] = {};
     double invader[kMaxN * kMaxN] = {};
 };
@@ -38,6 +39,7 @@ struct Axis {
     bool active = false;
     double h = 1.0;
     std::vector<double> sd_faces;    // (N+2) x nf, ghost elements included
+    std::vector<double> sd_centers;  // (N+2) x n, sub-cell centres
     std::vector<double> fv_faces;    // fvn + 1
     std::vector<double> fv_centers;  // fvn
 };

@@ -9,8 +9,9 @@ overrides of the reference defaults, and stores, per case:
   manifest.json  the overrides, the output index and the SHA-256 of the
                  reference's raw output file
 It also records the SHA-256 of the reference's committed goldens
-(tests/goldens/ in the reference tree). Needs the reference tree; run once:
-    python tests/golden/make_fixtures.py
+(tests/goldens/ in the reference tree) and the induction solver's outputs
+(INDUCTION_CASES). Needs the reference tree; run once:
+    python tests/golden/make_fixtures.py [--induction]
 """
 import hashlib
 import json
@@ -69,6 +70,54 @@ GOLDENS = {
     "hydro_sd/W_cv_N8p3_1_0.dat": "reference golden: 3D sine wave, N=8, p=3, ADER, t=0.1",
     "induction_fv/B2_cv_N8p3_2_0.dat": "reference golden: 3D induction loop with fallback, t=0.2",
 }
+
+
+# the 3D induction solver (magnetic loop advected at v = (1, 1, 0),
+# src/induction_ader.hpp): the reference golden deck (sha only) and small
+# variants; stored per case: the full B2_cv file (ghost elements included)
+# and, with the FV path, the full troubles file of the last output
+INDUCTION_BASE = ["job/system=induction", "induction/nu=0.0025", "time/cfl=0.8"]
+INDUCTION_CASES = {
+    "ind_golden_n8": ["job/fallback=true", "mesh/p=3", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=8",
+                      "time/tlim=0.2", "output/dt=0.1"],
+    "ind_n4_p3_ader": ["job/fallback=false", "mesh/p=3", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=4",
+                       "time/tlim=0.1", "output/dt=0.05"],
+    "ind_n6_p3_rk2_fv": ["job/fallback=true", "mesh/p=3", "mesh/nx1=6", "mesh/nx2=6", "mesh/nx3=6",
+                         "time/integrator=rk2", "time/tlim=0.1", "output/dt=0.05"],
+    "ind_n4_p2_rk3": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=4",
+                      "time/integrator=rk3", "time/tlim=0.1", "output/dt=0.05"],
+    "ind_n4_p4_rk2_gradfree": ["job/fallback=false", "mesh/p=4", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=4",
+                               "time/integrator=rk2", "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree",
+                               "mesh/x3_bc=gradfree", "time/tlim=0.05", "output/dt=0.05"],
+}
+# (the reference's FV induction path writes past its FV arrays in the ghost
+# fill of staggered fields and crashes at N = 4 for p = 2..4; the FV cases
+# above are ones it completes)
+
+
+def induction_fixtures(manifest):
+    for name, ov in INDUCTION_CASES.items():
+        ov = INDUCTION_BASE + ov
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out + "/", OMP_NUM_THREADS="8")
+            r = subprocess.run([REF_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            files = [f for f in os.listdir(out) if f.startswith("B2_cv_")]
+            last = max(files, key=lambda f: int(f.split("_")[-2]))
+            idx = int(last.split("_")[-2])
+            steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            entry = {"overrides": ov, "output": last, "steps": steps,
+                     "sha256_B2_cv": sha256(os.path.join(out, last))}
+            tr = [f for f in os.listdir(out) if f.startswith("troubles_") and int(f.split("_")[-2]) == idx]
+            if tr:
+                entry["troubles_output"] = tr[0]
+                entry["sha256_troubles"] = sha256(os.path.join(out, tr[0]))
+            if name != "ind_golden_n8":
+                arrays = {"B2_cv": np.fromfile(os.path.join(out, last))}
+                if tr:
+                    arrays["troubles"] = np.fromfile(os.path.join(out, tr[0]))
+                np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+            manifest.setdefault("induction_cases", {})[name] = entry
+            print(name, last, steps, flush=True)
 
 
 def sha256(path):
@@ -142,6 +191,7 @@ def main():
                 "overrides": ov, "steps": nsteps, "slots": "rho, vx, vy, p",
                 "sha256_signed_zero_folded": hashlib.sha256(a4.tobytes()).hexdigest()}
             print(name, nsteps, flush=True)
+    induction_fixtures(manifest)
     for rel, what in GOLDENS.items():
         path = os.path.join(REF_TREE, "tests", "goldens", rel)
         if os.path.exists(path):
@@ -151,4 +201,12 @@ def main():
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    if "--induction" in sys.argv:
+        # regenerate only the induction fixtures, keeping the rest of the manifest
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            m = json.load(f)
+        induction_fixtures(m)
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(m, f, indent=1)
+    else:
+        sys.exit(main())

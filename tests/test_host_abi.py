@@ -20,9 +20,10 @@ HEADER = os.path.join(ROOT, "include", "spdk.h")
 
 
 PROTO_HEADER = os.path.join(ROOT, "include", "spdk_proto.h")
+INDUCTION_HEADER = os.path.join(ROOT, "include", "spdk_induction.h")
 
 
-def declared_functions(paths=(HEADER, PROTO_HEADER)):
+def declared_functions(paths=(HEADER, PROTO_HEADER, INDUCTION_HEADER)):
     names = set()
     for path in paths:
         text = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
