@@ -159,6 +159,10 @@ int spdk_build_matrices(int p, int ader, double* sp_to_fp, double* dfp_to_sp, do
  * configuration (src/initial_conditions.cpp:179-228) in the solver layout
  * [element][var][point]; count = elements * (ndim+2) * points. */
 int spdk_initial_wcv(const spdk_hydro_config* cfg, double* out, size_t count);
+/* spdk_fv_faces: the FV sub-cell face coordinates of one direction, ghost
+ * frame included (the reference's dimension::fv_faces, src/structs.hpp:40-75):
+ * count = N (p+1) + 5 for an active direction, 1 for an inactive one. */
+int spdk_fv_faces(int N, int p, double L, int active, double* out, size_t count);
 
 /* Allocation-free step. No counterpart in the reference: it serves callers
  * that cannot allocate device memory when they advance the solution -- a

@@ -47,6 +47,7 @@ def stale():
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(HERE, "driver", "spdk_run.cpp"))
     deps += [os.path.join(ROOT, "include", h) for h in ("spdk.h", "spdk_proto.h", "spdk_induction.h")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -77,6 +78,15 @@ def build(force=False, verbose=False, jobs=None):
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
     os.replace(tmp, LIB)
+    # the athinput-driven driver executable, linked against the library
+    drv = os.path.join(HERE, "spdk_run")
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+           os.path.join(HERE, "driver", "spdk_run.cpp"), "-o", drv + ".tmp",
+           "-L" + HERE, "-l:libspdk_cuda.so", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("driver build failed:\n" + r.stdout + r.stderr)
+    os.replace(drv + ".tmp", drv)
     return LIB
 
 

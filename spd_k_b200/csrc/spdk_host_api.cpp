@@ -43,3 +43,20 @@ extern "C" int spdk_initial_wcv(const spdk_hydro_config* cfg, double* out, size_
     std::memcpy(out, w.data(), sizeof(double) * w.size());
     return 0;
 }
+
+extern "C" int spdk_fv_faces(int N, int p, double L, int active, double* out, size_t count) {
+    if (!out || N < 1 || p < 1 || p > spdk::kMaxP || !(L > 0)) return spdk::fail(SPDK_E_ARG, "bad argument");
+    spdk::Matrices m;
+    spdk::build_matrices(p, true, &m);
+    if (!active) {
+        // one face at (0 - NGH + x_fp[0]) h, h = L (src/structs.hpp:60-63)
+        if (count != 1) return spdk::fail(SPDK_E_ARG, "count must be 1 for an inactive direction");
+        out[0] = (0 + 0 - 1 + m.x_fp[0]) * L;
+        return 0;
+    }
+    spdk::Axis a;
+    spdk::build_axis(N, p, L, m.x_fp, true, &a);
+    if (count != a.fv_faces.size()) return spdk::fail(SPDK_E_ARG, "count must be " + std::to_string(a.fv_faces.size()));
+    std::memcpy(out, a.fv_faces.data(), sizeof(double) * a.fv_faces.size());
+    return 0;
+}

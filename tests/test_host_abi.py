@@ -125,3 +125,33 @@ def test_initial_condition_matches_oracle(lib, ov):
     mine = out.reshape(Nz, Ny, Nx, V, nz, n, n).transpose(3, 0, 1, 2, 4, 5, 6)
     slots = [0, 1, 2, 3, 4] if D == 3 else [0, 1, 2, 4]
     assert np.array_equal(mine, w[slots])
+
+
+def test_driver_rejects_bad_command_lines_without_a_device(tmp_path):
+    """spdk_run parses like src/main.cpp: -i <deck>, block/name=value
+    overrides, anything else is an error; configuration errors end the run
+    before any device call"""
+    import subprocess
+    drv = os.path.join(ROOT, "spd_k_b200", "spdk_run")
+    env = dict(os.environ, SPD_OUTPUT_DIR=str(tmp_path))
+    for args, msg in ((["bogus"], "unrecognized argument"), (["job/system=mhd"], "unknown system"),
+                      (["mesh/nx1=1"], "x-direction must be active"),
+                      (["time/integrator=rk4"], "unknown integrator"),
+                      (["mesh/x1_bc=open"], "unknown boundary"),
+                      (["-i", str(tmp_path / "missing.athinput")], "cannot open input file")):
+        r = subprocess.run([drv] + args, capture_output=True, text=True, env=env, timeout=60)
+        assert r.returncode == 1 and msg in r.stderr, (args, r.stderr)
+
+
+def test_fv_faces_match_oracle(lib):
+    from oracle import oracle as O
+    c = oracle_config(["mesh/nx1=6", "mesh/nx2=4", "mesh/nx3=1", "mesh/x1len=0.3", "mesh/p=4"])
+    o = O.Oracle(c)
+    for d, (N, L, act) in enumerate(((6, 0.3, 1), (4, 1.0, 1), (1, 1.0, 0))):
+        want = o.array("fv_faces_" + "xyz"[d]).reshape(-1)
+        n = len(want) if act else 1
+        out = np.zeros(n)
+        assert lib.spdk_fv_faces(N, 4, ctypes.c_double(L), act, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 ctypes.c_size_t(n)) == 0
+        if act:
+            assert np.array_equal(out, want)
