@@ -12,7 +12,15 @@ A step is one full ADER step (p+1 Picard passes + p+1 fallback slices +
 dt reduction). The metric is DOF-updates/s = active solution points x steps
 / seconds (the reference's "zone-cycles/s", src/hydro_ader.hpp:263-271).
 
+The timed form is, by default, the mixed + learned form: FP32 state,
+transforms and fluxes with FP64 islands (pressure recovery, detector bounds,
+dt) and the learned a-priori indicator (spd_k_b200/data/indicator_2d_p3.npz)
+flagging elements for the fallback every step. The plain FP64 form (the
+reference's arithmetic, bit-identical to it) and the mixed form without the
+indicator are timed beside it on the same workload.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--precision fp32|fp64] [--learned PATH|none]
 
 N>1 runs N independent replicas (one per GPU, weak scaling); the headline
 time is the max over ranks of CUDA-event time on each solver stream.
@@ -34,6 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "blast2d-256x256-p3-ader-nad-muscl"
+DEFAULT_INDICATOR = os.path.join(ROOT, "spd_k_b200", "data", "indicator_2d_p3.npz")
 P0_BLAST = 0.4 / (math.pi * 0.01 ** 2)  # (gamma-1) E / (pi r^2), E = 1, r = 0.01
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
@@ -272,8 +281,11 @@ def main():
     ap.add_argument("--N", type=int, default=256)
     ap.add_argument("--no-graph", action="store_true",
                     help="launch the timed steps one by one instead of replaying the step graph")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                    help="arithmetic of the timed form; fp32 also times the plain fp64 form beside it")
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
+                    help="arithmetic of the timed form (the plain fp64 form is timed beside any other)")
+    ap.add_argument("--learned", default=DEFAULT_INDICATOR,
+                    help="weights of the learned a-priori indicator ('none': without it)")
+    ap.add_argument("--threshold", type=float, default=0.5)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -288,10 +300,22 @@ def main():
 
     c = dict(workload_config(args.N), precision=args.precision)
     esz = 4 if args.precision == "fp32" else 8
+    learned = args.learned and args.learned != "none"
+    ind = None
+    if learned:
+        from spd_k_b200.learned import Indicator, set_indicator
+        torch_dev = f"cuda:{local}"
+        import torch
+        torch.cuda.set_device(local)
+        ind = Indicator.load(args.learned)
     solver = S.HydroSolver(c, device=local)
+    if ind is not None:
+        set_indicator(solver, ind, args.threshold)
     L = S.load_library()
     info = solver.info
     dof = info.n_dof
+    form = ("mixed+learned" if learned else "mixed") if args.precision == "fp32" else (
+        "plain+learned" if learned else "plain")
 
     # ---- headline: K graph-replayed steps, inputs resident in HBM ----
     import torch
@@ -354,6 +378,8 @@ def main():
 
     # ---- e2e through the C ABI with host buffers (reference driver loop) ----
     solver2 = S.HydroSolver(c, device=local)
+    if ind is not None:
+        set_indicator(solver2, ind, args.threshold)
     u_host = torch.empty(info.n_elements * info.nvar * info.n_points, dtype=torch.float64,
                          pin_memory=True).numpy()   # the C ABI exchanges doubles in both forms
     solver2.read(S.FIELD_U_SP, out=u_host)
@@ -380,27 +406,27 @@ def main():
            "steps": e2e_steps, "path": "spdk_hydro_write + spdk_hydro_step/get_dt per step + spdk_hydro_read"}
     solver2.close()
 
-    # ---- the plain FP64 form on the same workload, beside the precision form ----
-    plain = None
-    if args.precision != "fp64":
-        c64 = dict(c, precision="fp64")
-        s64 = S.HydroSolver(c64, device=local)
-        rc = L.spdk_hydro_get_stream(s64.h, ctypes.byref(sp))
-        st64 = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
-        s64.steps(args.warmup)
-        s64.sync()
+    # ---- the other forms on the same workload, beside the timed one ----
+    def time_form(cf):
+        sv = S.HydroSolver(cf, device=local)
+        rc = L.spdk_hydro_get_stream(sv.h, ctypes.byref(sp))
+        st = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
+        sv.steps(args.warmup)
+        sv.sync()
         barrier(dist)
         g0 = torch.cuda.Event(enable_timing=True)
         g1 = torch.cuda.Event(enable_timing=True)
-        g0.record(st64)
-        s64.steps(args.steps)
-        g1.record(st64)
+        g0.record(st)
+        sv.steps(args.steps)
+        g1.record(st)
         g1.synchronize()
-        ms64 = max_over_ranks(dist, g0.elapsed_time(g1), f"cuda:{local}")
-        plain = {"value": aggregate_throughput(world, dof, args.steps, ms64), "unit": "DOF-updates/s",
-                 "ms_per_step": ms64 / args.steps, "steps": args.steps,
-                 "speedup": (ms64 / args.steps) / (ms / args.steps)}
-        s64.close()
+        msf = max_over_ranks(dist, g0.elapsed_time(g1), f"cuda:{local}")
+        sv.close()
+        return {"value": aggregate_throughput(world, dof, args.steps, msf), "unit": "DOF-updates/s",
+                "ms_per_step": msf / args.steps, "steps": args.steps,
+                "timed_form_speedup": (msf / args.steps) / (ms / args.steps)}
+    plain = time_form(dict(c, precision="fp64")) if (args.precision != "fp64" or learned) else None
+    mixed = time_form(dict(c, precision="fp32")) if (args.precision == "fp32" and learned) else None
 
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
@@ -419,12 +445,16 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (f64 islands)" if args.precision == "fp32" else "f64",
+            "form": form,
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "elements": [args.N, args.N], "p": 3, "dof_per_gpu": dof,
                        "integrator": "ader", "riemann": "LLF at SD faces, HLLC at fallback faces",
                        "fallback": "NAD(1e-5, Moore)+SED+PAD, theta-blended MUSCL-Hancock",
                        "precision": ("fp32 state/transforms/fluxes; fp64 pressure recovery, detector bounds, dt"
                                      if args.precision == "fp32" else "fp64, reference operation order (plain form)"),
+                       "learned_indicator": (f"BF16 MLP {os.path.relpath(args.learned, ROOT)}, threshold "
+                                             f"{args.threshold}: a-priori fallback flags every step"
+                                             if learned else None),
                        "parallelism": f"replicas{world}",
                        "l2": f"no flush: device working set {state_gb:.2f} GB > 126 MB L2",
                        "state": "steps continue from the initial blast after the warm-up"},
@@ -433,11 +463,14 @@ def main():
             "kernels": kernel_table,
             "e2e": e2e,
             "plain_fp64": plain,
+            "mixed_without_indicator": mixed,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     solver.close()
+    if ind is not None:
+        ind.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0

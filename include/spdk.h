@@ -101,7 +101,9 @@ enum {
     SPDK_FIELD_U_SP = 0,      /* conserved state at solution points */
     SPDK_FIELD_W_CV = 1,      /* primitive sub-cell averages (written every step) */
     SPDK_FIELD_TROUBLES = 2,  /* last fallback slice's trouble flags, 0/1 per sub-cell */
-    SPDK_FIELD_THETA = 3      /* last fallback slice's blending factor per sub-cell */
+    SPDK_FIELD_THETA = 3,     /* last fallback slice's blending factor per sub-cell */
+    SPDK_FIELD_ELEMENT_TROUBLES = 4,  /* per element: 1 if NAD/SED/PAD flagged a sub-cell in any slice of the last step */
+    SPDK_FIELD_ELEMENT_PREDICTED = 5  /* per element: the learned indicator's a-priori flag of the last step */
 };
 
 const char* spdk_last_error(void);

@@ -23,6 +23,7 @@ PROBLEMS = {
     "rti_top": 12,
 }
 FIELD_U_SP, FIELD_W_CV, FIELD_TROUBLES, FIELD_THETA = 0, 1, 2, 3
+FIELD_ELEMENT_TROUBLES, FIELD_ELEMENT_PREDICTED = 4, 5
 # arithmetic of the solver: the plain FP64 form (bitwise the reference) or
 # the FP32 precision form (FP64 kept for pressure recovery, detector bounds, dt)
 PRECISIONS = {"fp64": 0, "fp32": 1}
@@ -278,7 +279,12 @@ class HydroSolver:
 
     def read(self, field, out=None):
         cells = self.info.n_elements * self.npt
-        count = cells * self.nvar if field in (FIELD_U_SP, FIELD_W_CV) else cells
+        if field in (FIELD_U_SP, FIELD_W_CV):
+            count = cells * self.nvar
+        elif field in (FIELD_ELEMENT_TROUBLES, FIELD_ELEMENT_PREDICTED):
+            count = self.info.n_elements
+        else:
+            count = cells
         a = out if out is not None else np.empty(count, dtype=np.float64)
         _check(_lib.spdk_hydro_read(self.h, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), count))
         return a

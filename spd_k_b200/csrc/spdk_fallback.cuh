@@ -203,6 +203,9 @@ __global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const do
         const double rho = here_new.x, p = here_new.y;
         if (rho < kRhoMin || rho > kRhoMax) tr = 1;
         if (p < kPMin || p > kPMax) tr = 1;
+        const long long el = cid / NPT;
+        if (G.elem_trouble && tr > 0) G.elem_trouble[el] = 1;  // a-posteriori label
+        if (G.elem_pred && G.elem_pred[el]) tr = 1;            // a-priori prediction
         T[cid] = tr > 0 ? 1 : 0;
         if (any_trouble && tr > 0) atomicAdd(any_trouble, 1);
     }

@@ -9,6 +9,8 @@
 #include <vector>
 
 #include "spdk.h"
+#include "spdk_learned.h"
+#include "spdk_learned_impl.h"
 #include "spdk_kernelset.cuh"
 #include "spdk_setup.h"
 
@@ -57,6 +59,12 @@ struct spdk_hydro {
     uint8_t *trouble = nullptr, *theta = nullptr;
     unsigned long long* dtmin = nullptr;
     int* status = nullptr;  // device-detected faults (kStatus* bits)
+    // learned indicator: per-element labels, predictions, feature rows
+    uint8_t *elem_trouble = nullptr, *elem_pred = nullptr;
+    uint16_t* feat = nullptr;
+    float2* means = nullptr;
+    spdk_mlp* mlp = nullptr;
+    float thr = 0.5f;
     size_t bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -216,8 +224,18 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
 }
 
 int enqueue_step(spdk_hydro* h) {
-    return h->prec == SPDK_PRECISION_FP32 ? enqueue_step_t<float>(h, h->ks32, h->dm32)
-                                          : enqueue_step_t<double>(h, h->ks64, h->dm64);
+    if (h->elem_trouble) SPDK_CUDA(cudaMemsetAsync(h->elem_trouble, 0, (size_t)h->E, h->stream));
+    if (h->mlp) {
+        // a-priori indicator on the state at the start of the step
+        const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
+        int rc = feature_rows(h->u, h->prec == SPDK_PRECISION_FP32, h->D, h->p, N, h->G.bc, h->G.gm, h->E, h->means,
+                              h->feat, h->stream);
+        if (!rc) rc = mlp_infer_flags(h->mlp, h->feat, h->E, nullptr, h->elem_pred, h->thr, h->stream);
+        if (rc) return rc;
+    }
+    const int rc = h->prec == SPDK_PRECISION_FP32 ? enqueue_step_t<float>(h, h->ks32, h->dm32)
+                                                  : enqueue_step_t<double>(h, h->ks64, h->dm64);
+    return rc;
 }
 
 __global__ void narrow_kernel(const double* __restrict__ a, float* __restrict__ b, long long n) {
@@ -248,7 +266,8 @@ void release(spdk_hydro* h) {
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
                     h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
-                    h->rpo, h->rpn, h->trouble, h->theta, h->dtmin, h->status};
+                    h->rpo, h->rpn, h->trouble, h->theta, h->dtmin, h->status, h->elem_trouble, h->elem_pred,
+                    h->feat, h->means};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -380,6 +399,9 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         if (!rc) rc = dalloc(h, (void**)&h->rpn, (size_t)h->E * h->NPT * sizeof(double2));
         if (!rc) rc = dalloc(h, (void**)&h->trouble, (size_t)h->E * h->NPT);
         if (!rc) rc = dalloc(h, (void**)&h->theta, (size_t)h->E * h->NPT);
+        if (!rc) rc = dalloc(h, (void**)&h->elem_trouble, (size_t)h->E);
+        if (!rc && cudaMemset(h->elem_trouble, 0, (size_t)h->E) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset");
+        G.elem_trouble = h->elem_trouble;
         for (int d = 0; d < D && !rc; d++) {
             rc = dalloc(h, (void**)&h->fvf[d], h->ax[d].fv_faces.size() * sizeof(double));
             if (!rc) rc = dalloc(h, (void**)&h->fvc[d], h->ax[d].fv_centers.size() * sizeof(double));
@@ -456,7 +478,7 @@ int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info) {
     info->n_time_slices = h->nt;
     int l = 0;
     for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 3 * h->nt : 1);
-    info->launches_per_step = l + 1;
+    info->launches_per_step = l + 1 + (h->mlp ? 3 : 0);
     info->device_bytes = h->bytes;
     return 0;
 }
@@ -583,6 +605,17 @@ int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count) {
         SPDK_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     }
+    if (field == SPDK_FIELD_ELEMENT_TROUBLES || field == SPDK_FIELD_ELEMENT_PREDICTED) {
+        if (!h->cfg.fallback) return fail(SPDK_E_STATE, "fallback is off");
+        const uint8_t* src = field == SPDK_FIELD_ELEMENT_TROUBLES ? h->elem_trouble : h->elem_pred;
+        if (!src) return fail(SPDK_E_STATE, "no indicator set");
+        if (count != (size_t)h->E) return fail(SPDK_E_ARG, "count must be the number of elements");
+        std::vector<uint8_t> b(h->E);
+        SPDK_CUDA(cudaMemcpyAsync(b.data(), src, h->E, cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaStreamSynchronize(h->stream));
+        for (long long q = 0; q < h->E; q++) host[q] = b[q];
+        return 0;
+    }
     if (field == SPDK_FIELD_TROUBLES || field == SPDK_FIELD_THETA) {
         if (!h->cfg.fallback) return fail(SPDK_E_STATE, "fallback is off");
         if (count != cells) return fail(SPDK_E_ARG, "count must be E*NPT = " + std::to_string(cells));
@@ -622,6 +655,52 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
     SPDK_CUDA(cudaGetLastError());
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int spdk_hydro_feature_size(spdk_hydro* h, int* n_in) {
+    if (!h || !n_in) return fail(SPDK_E_ARG, "null argument");
+    *n_in = 2 * h->NPT + 4 * h->D;
+    return 0;
+}
+
+int spdk_hydro_features(spdk_hydro* h, uint16_t* x, size_t count) {
+    if (!h || !x) return fail(SPDK_E_ARG, "null argument");
+    const size_t need = (size_t)h->E * (2 * h->NPT + 4 * h->D);
+    if (count != need) return fail(SPDK_E_ARG, "count must be " + std::to_string(need));
+    if (!h->means && dalloc(h, (void**)&h->means, (size_t)h->E * sizeof(float2))) return fail(SPDK_E_NOMEM, "means");
+    const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
+    return feature_rows(h->u, h->prec == SPDK_PRECISION_FP32, h->D, h->p, N, h->G.bc, h->G.gm, h->E, h->means, x,
+                        h->stream);
+}
+
+int spdk_hydro_set_indicator(spdk_hydro* h, spdk_mlp* m, float threshold) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    if (m && !h->cfg.fallback) return fail(SPDK_E_STATE, "the indicator feeds the fallback: set fallback = 1");
+    if (m && mlp_n_in(m) != 2 * h->NPT + 4 * h->D)
+        return fail(SPDK_E_ARG, "the network's input size does not match this solver's feature rows");
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    if (m) {
+        if (!h->feat && dalloc(h, (void**)&h->feat, (size_t)h->E * (2 * h->NPT + 4 * h->D) * sizeof(uint16_t)))
+            return fail(SPDK_E_NOMEM, "features");
+        if (!h->means && dalloc(h, (void**)&h->means, (size_t)h->E * sizeof(float2))) return fail(SPDK_E_NOMEM, "means");
+        if (!h->elem_pred) {
+            if (dalloc(h, (void**)&h->elem_pred, (size_t)h->E)) return fail(SPDK_E_NOMEM, "predictions");
+            SPDK_CUDA(cudaMemset(h->elem_pred, 0, (size_t)h->E));
+        }
+    }
+    h->mlp = m;
+    h->thr = threshold;
+    h->G.elem_pred = m ? h->elem_pred : nullptr;
+    // the captured step holds the old kernel arguments
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
     return 0;
 }
 

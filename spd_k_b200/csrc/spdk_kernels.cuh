@@ -55,6 +55,11 @@ struct DevGrid {
     // fallback settings
     double nad_tol;
     int nad_delta, nad_moore, use_sed, blending;
+    // learned indicator: per element, set when NAD/SED/PAD flags any of its
+    // sub-cells in any slice of the step (NULL: not recorded), and the
+    // a-priori prediction that counts all its sub-cells troubled (NULL: off)
+    uint8_t* elem_trouble;
+    const uint8_t* elem_pred;
 };
 
 enum { kPredict = 0, kCorrect = 1, kFlux = 2 };
