@@ -241,7 +241,26 @@ class HydroSolver:
         self.t = 0.0
         self.n_step = 0
 
+    @classmethod
+    def attach(cls, handle, c):
+        """a non-owning view of a solver handle owned elsewhere (a batch member)"""
+        self = cls.__new__(cls)
+        self.c = c
+        self.h = handle
+        self._owner = False
+        info = HydroInfo()
+        _check(_lib.spdk_hydro_get_info(self.h, ctypes.byref(info)))
+        self.info = info
+        self.ndim, self.p, self.npt, self.nvar = info.ndim, info.p, info.n_points, info.nvar
+        self.N = tuple(info.N)
+        self.t = 0.0
+        self.n_step = 0
+        return self
+
     def close(self):
+        if not getattr(self, "_owner", True):
+            self.h = None
+            return
         if getattr(self, "h", None):
             _lib.spdk_hydro_destroy(self.h)
             self.h = None

@@ -1,0 +1,87 @@
+"""Python binding of the batched form (include/spdk_batch.h)."""
+import ctypes
+
+from .api import HydroConfig, HydroSolver, SpdkError, load_library, make_config
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_problems", ctypes.c_int), ("n_groups", ctypes.c_int), ("n_dof", ctypes.c_longlong),
+        ("launches_per_step", ctypes.c_int), ("group_p", ctypes.c_int * 8), ("group_tile", ctypes.c_int * 8),
+        ("group_size", ctypes.c_int * 8), ("device_bytes", ctypes.c_size_t),
+    ]
+
+
+def _lib():
+    L = load_library()
+    if not getattr(L, "_batch_types", False):
+        vp = ctypes.c_void_p
+        L.spdk_batch_create.argtypes = [ctypes.POINTER(HydroConfig), ctypes.c_int, ctypes.POINTER(vp)]
+        L.spdk_batch_destroy.argtypes = [vp]
+        L.spdk_batch_autotune.argtypes = [vp, ctypes.c_int]
+        L.spdk_batch_steps.argtypes = [vp, ctypes.c_int]
+        L.spdk_batch_sync.argtypes = [vp]
+        L.spdk_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
+        L.spdk_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.spdk_batch_member.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L._batch_types = True
+    return L
+
+
+def _check(L, rc):
+    if rc != 0:
+        raise SpdkError(f"spdk error {rc}: {L.spdk_last_error().decode()}")
+
+
+class Batch:
+    """Many independent 2D problems (configuration dicts) stepped together."""
+
+    def __init__(self, configs, device=0):
+        L = _lib()
+        self.configs = list(configs)
+        arr = (HydroConfig * len(self.configs))(*[make_config(c, device) for c in self.configs])
+        h = ctypes.c_void_p()
+        _check(L, L.spdk_batch_create(arr, len(self.configs), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().spdk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self, steps=3):
+        L = _lib()
+        _check(L, L.spdk_batch_autotune(self.h, steps))
+
+    def steps(self, n):
+        L = _lib()
+        _check(L, L.spdk_batch_steps(self.h, n))
+
+    def sync(self):
+        L = _lib()
+        _check(L, L.spdk_batch_sync(self.h))
+
+    def info(self):
+        L = _lib()
+        i = BatchInfo()
+        _check(L, L.spdk_batch_get_info(self.h, ctypes.byref(i)))
+        return i
+
+    def stream(self):
+        L = _lib()
+        s = ctypes.c_void_p()
+        _check(L, L.spdk_batch_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def member(self, i):
+        """a read-only solver view of problem i (read after sync())"""
+        L = _lib()
+        m = ctypes.c_void_p()
+        _check(L, L.spdk_batch_member(self.h, i, ctypes.byref(m)))
+        return HydroSolver.attach(m, self.configs[i])

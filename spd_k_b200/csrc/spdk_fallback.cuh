@@ -118,9 +118,9 @@ __device__ __forceinline__ double sed_component(const DevGrid& G, const double2*
 // kernel; the detector computes in FP64 in both, and a separate
 // instantiation per form keeps each form's compile flags on its own copy.
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
+__device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
-                                                            uint8_t* __restrict__ T, int* any_trouble) {
+                                                            uint8_t* __restrict__ T, int* any_trouble, long long bidx) {
     constexpr int n = P + 1;
     constexpr int NPT = Shape<D, P>::NPT;
     constexpr int Bx = TX * n, By = TY * n, Bz = D == 3 ? TZ * n : 1;
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const do
     const int dz = D == 3 ? 1 : 0;
     int o[3];
     {
-        int b = blockIdx.x;
+        int b = bidx;
         const int tx = G.N[0] / TX, ty = G.N[1] / TY;
         o[0] = (b % tx) * Bx;
         b /= tx;
@@ -211,6 +211,13 @@ __global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const do
     }
 }
 
+template <typename R, int D, int P, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
+                                                            const double2* __restrict__ rpn,
+                                                            uint8_t* __restrict__ T, int* any_trouble) {
+    fv_detect_kernel_body<R, D, P, TX, TY, TZ>(G, rpo, rpn, T, any_trouble, blockIdx.x);
+}
+
 // cell box of an element tile with a halo of g cells per active side
 template <int D, int P, int TX, int TY, int TZ>
 struct CellBox {
@@ -225,8 +232,8 @@ struct CellBox {
 // (src/trouble_detection.cpp:191-242); theta_from_troubles without blending
 // ---------------------------------------------------------------------------
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uint8_t* __restrict__ T,
-                                                           uint8_t* __restrict__ theta) {
+__device__ __forceinline__ void fv_theta_kernel_body(const DevGrid& G, const uint8_t* __restrict__ T,
+                                                           uint8_t* __restrict__ theta, long long bidx) {
     constexpr int n = P + 1;
     using CB = CellBox<D, P, TX, TY, TZ>;
     constexpr int E2x = TX * n + 4, E2y = TY * n + 4, E2z = D == 3 ? TZ * n + 4 : 1;
@@ -235,7 +242,7 @@ __global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uin
     __shared__ float Th[E1x * E1y * E1z];
     int o[3];
     {
-        int b = blockIdx.x;
+        int b = bidx;
         const int tx = G.N[0] / TX, ty = G.N[1] / TY;
         o[0] = (b % tx) * TX * n;
         b /= tx;
@@ -289,6 +296,12 @@ __global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uin
         int ga[3] = {o[0] + x - 1, o[1] + y - 1, o[2] + z - dz};
         theta[cell_id<D, P>(G, ga)] = (uint8_t)(t * 8.0f);
     }
+}
+
+template <typename R, int D, int P, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uint8_t* __restrict__ T,
+                                                           uint8_t* __restrict__ theta) {
+    fv_theta_kernel_body<R, D, P, TX, TY, TZ>(G, T, theta, blockIdx.x);
 }
 
 // MUSCL-Hancock face states of cell X for a face of direction Dn
@@ -352,7 +365,7 @@ struct UpdateSmem {
 // U_sp = cv_to_sp(U_cv), the RK combination, W_cv and the next dt.
 // ---------------------------------------------------------------------------
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+__device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const DevMatsT<R>& M, const FallbackArgsT<R>& A, long long bidx) {
     using SM = UpdateSmem<R, D, P, TX, TY, TZ>;
     constexpr int n = P + 1, nf = P + 2, V = D + 2, NPT = SM::NPT, NFP = Shape<D, P>::NFP;
     constexpr int Bx = SM::Bx, By = SM::By, Bz = SM::Bz, NC = SM::NC;
@@ -368,7 +381,7 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT
 
     int o[3], oe[3];
     {
-        int b = blockIdx.x;
+        int b = bidx;
         const int tx = G.N[0] / TX, ty = G.N[1] / TY;
         oe[0] = (b % tx) * TX;
         b /= tx;
@@ -597,6 +610,11 @@ __global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT
         }
         block_min_dt(dtl, A.dtmin);
     }
+}
+
+template <typename R, int D, int P, int TX, int TY, int TZ>
+__global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+    fv_update_kernel_body<R, D, P, TX, TY, TZ>(G, M, A, blockIdx.x);
 }
 
 }  // namespace spdk

@@ -34,47 +34,7 @@ int fail(int code, const std::string& msg) {
 
 using namespace spdk;
 
-struct spdk_hydro {
-    spdk_hydro_config cfg{};
-    int D = 2, p = 3, n = 4, nf = 5, V = 4, NPT = 16, nt = 4, nstages = 1;
-    double rk_a[3] = {0, 0, 0};
-    long long E = 0;
-    Matrices mats;
-    Axis ax[3];
-    int prec = SPDK_PRECISION_FP64;
-    size_t esz = sizeof(double);       // bytes per state value
-    DevMatsT<double> dm64{};
-    DevMatsT<float> dm32{};
-    DevGrid G{};
-    KernelSetT<double> ks64;           // FP64 kernels (also the FP32 form's set-up)
-    KernelSetT<float> ks32;
-    int tile[3] = {1, 1, 1};
-    cudaStream_t stream = nullptr;
-    // state buffers hold doubles (plain form) or floats (precision form)
-    void *u = nullptr, *ua[2] = {nullptr, nullptr}, *u0 = nullptr, *ucv[2] = {nullptr, nullptr};
-    void *ff[3] = {nullptr, nullptr, nullptr}, *wcv = nullptr;
-    double* dt = nullptr;
-    double *fvf[3] = {nullptr, nullptr, nullptr}, *fvc[3] = {nullptr, nullptr, nullptr};
-    double2 *rpo = nullptr, *rpn = nullptr;
-    uint8_t *trouble = nullptr, *theta = nullptr;
-    unsigned long long* dtmin = nullptr;
-    int* status = nullptr;  // device-detected faults (kStatus* bits)
-    // learned indicator: per-element labels, predictions, feature rows
-    uint8_t *elem_trouble = nullptr, *elem_pred = nullptr;
-    uint16_t* feat = nullptr;
-    float2* means = nullptr;
-    spdk_mlp* mlp = nullptr;
-    float thr = 0.5f;
-    size_t bytes = 0;
-    cudaGraphExec_t graph = nullptr;
-    int graph_steps = 0;
-    int launches = 0;
-    // per-launch event timing (spdk_hydro_profile)
-    bool profiling = false;
-    std::vector<cudaEvent_t> ev;
-    std::vector<int> ev_kind;
-    size_t ev_used = 0;
-};
+#include "spdk_hydro_impl.h"
 
 namespace {
 
@@ -179,6 +139,10 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
             prof_end(h, SPDK_KERNEL_FLUX);
             launches++;
+            if (h->join_pending) {
+                SPDK_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+                h->join_pending = false;
+            }
             for (int t = 0; t < h->nt; t++) {
                 prof_begin(h);
                 k.detect<<<blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
@@ -226,12 +190,17 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
 int enqueue_step(spdk_hydro* h) {
     if (h->elem_trouble) SPDK_CUDA(cudaMemsetAsync(h->elem_trouble, 0, (size_t)h->E, h->stream));
     if (h->mlp) {
-        // a-priori indicator on the state at the start of the step
+        // a-priori indicator on the state at the start of the step, on the
+        // side stream (U is not written before the first detection)
+        SPDK_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+        SPDK_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
         const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
         int rc = feature_rows(h->u, h->prec == SPDK_PRECISION_FP32, h->D, h->p, N, h->G.bc, h->G.gm, h->E, h->means,
-                              h->feat, h->stream);
-        if (!rc) rc = mlp_infer_flags(h->mlp, h->feat, h->E, nullptr, h->elem_pred, h->thr, h->stream);
+                              h->feat, h->side);
+        if (!rc) rc = mlp_infer_flags(h->mlp, h->feat, h->E, nullptr, h->elem_pred, h->thr, h->side);
         if (rc) return rc;
+        SPDK_CUDA(cudaEventRecord(h->ev_join, h->side));
+        h->join_pending = true;
     }
     const int rc = h->prec == SPDK_PRECISION_FP32 ? enqueue_step_t<float>(h, h->ks32, h->dm32)
                                                   : enqueue_step_t<double>(h, h->ks64, h->dm64);
@@ -270,6 +239,9 @@ void release(spdk_hydro* h) {
                     h->feat, h->means};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -685,6 +657,11 @@ int spdk_hydro_set_indicator(spdk_hydro* h, spdk_mlp* m, float threshold) {
         return fail(SPDK_E_ARG, "the network's input size does not match this solver's feature rows");
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
     if (m) {
+        if (!h->side) {
+            SPDK_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+            SPDK_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+            SPDK_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+        }
         if (!h->feat && dalloc(h, (void**)&h->feat, (size_t)h->E * (2 * h->NPT + 4 * h->D) * sizeof(uint16_t)))
             return fail(SPDK_E_NOMEM, "features");
         if (!h->means && dalloc(h, (void**)&h->means, (size_t)h->E * sizeof(float2))) return fail(SPDK_E_NOMEM, "means");

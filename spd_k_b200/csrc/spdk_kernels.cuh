@@ -486,7 +486,7 @@ constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? 3 : 2;
 // fused so that only U_ader crosses HBM.
 // ---------------------------------------------------------------------------
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
-__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+__device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMatsT<R>& M, const PicardArgsT<R>& A, long long bidx) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_
     const int tid = threadIdx.x;
     int o[3];
     {
-        int b = blockIdx.x;
+        int b = bidx;
         const int tx = G.N[0] / TX, ty = G.N[1] / TY;
         o[0] = (b % tx) * TX;
         b /= tx;
@@ -865,6 +865,11 @@ __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_
             A.rp_new[ge * NPT + pt] = rho_p_fp64<D>(un, G.gm);
         }
     }
+}
+
+template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
+__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+    picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(G, M, A, blockIdx.x);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>

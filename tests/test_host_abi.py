@@ -22,9 +22,10 @@ HEADER = os.path.join(ROOT, "include", "spdk.h")
 PROTO_HEADER = os.path.join(ROOT, "include", "spdk_proto.h")
 INDUCTION_HEADER = os.path.join(ROOT, "include", "spdk_induction.h")
 LEARNED_HEADER = os.path.join(ROOT, "include", "spdk_learned.h")
+BATCH_HEADER = os.path.join(ROOT, "include", "spdk_batch.h")
 
 
-def declared_functions(paths=(HEADER, PROTO_HEADER, INDUCTION_HEADER, LEARNED_HEADER)):
+def declared_functions(paths=(HEADER, PROTO_HEADER, INDUCTION_HEADER, LEARNED_HEADER, BATCH_HEADER)):
     names = set()
     for path in paths:
         text = re.sub(r"/\*.*?\*/", "", open(path).read(), flags=re.S)
