@@ -249,6 +249,62 @@ def barrier(dist):
         dist.barrier()
 
 
+def batched_configs(count, seed=2024, precision="fp32"):
+    """seeded ensemble of four-quadrant Riemann problems: element counts per
+    side uniform in {16, 24, ..., 64}, p uniform in {2, 3, 5}, rho and P in
+    U[0.1, 1], v in U[-1, 1], gamma 1.4, HLLC + NAD/MUSCL fallback, outflow"""
+    import numpy as np
+    from spd_k_b200.api import apply_overrides, config_from_params
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx, ny = (int(v) for v in rng.integers(2, 9, 2) * 8)
+        p = int(rng.choice([2, 3, 5]))
+        ov = ["job/fallback=true", f"mesh/p={p}", f"mesh/nx1={nx}", f"mesh/nx2={ny}", "mesh/nx3=1",
+              "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "problem/problem=quadrant", "hydro/gamma=1.4",
+              "output/dt=-1"]
+        c = config_from_params(apply_overrides({}, ov))
+        q = []
+        for _ in range(4):
+            q += [rng.uniform(0.1, 1.0), rng.uniform(0.1, 1.0), rng.uniform(-1, 1), rng.uniform(-1, 1)]
+        c["q"] = q
+        c["precision"] = precision
+        out.append(c)
+    return out
+
+
+def batched_leg(args, local, dist, world):
+    """the batched form on the ensemble: autotuned tiles, graph-replayed
+    steps, DOF-updates/s of all problems together"""
+    import ctypes
+    import torch
+    import spd_k_b200.batch as B
+    b = B.Batch(batched_configs(args.batch_problems), device=local)
+    b.autotune(2)
+    info = b.info()
+    st = torch.cuda.ExternalStream(b.stream(), device=f"cuda:{local}")
+    b.steps(3)
+    b.sync()
+    barrier(dist)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    b.steps(args.batch_steps)
+    e1.record(st)
+    e1.synchronize()
+    b.sync()
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), f"cuda:{local}")
+    res = {"value": aggregate_throughput(world, info.n_dof, args.batch_steps, ms), "unit": "DOF-updates/s",
+           "problems": info.n_problems, "dof": info.n_dof, "steps": args.batch_steps,
+           "ms_per_step": ms / args.batch_steps, "launches_per_step": info.launches_per_step,
+           "groups": {int(info.group_p[g]): {"problems": int(info.group_size[g]), "tile": int(info.group_tile[g])}
+                      for g in range(info.n_groups)},
+           "workload": "four-quadrant Riemann ensemble, N per side in {16..64} step 8, p in {2,3,5}, FP32 form, "
+                       "ADER + NAD/MUSCL, autotuned tiles, graph-captured step"}
+    b.close()
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
                                 int(os.environ.get("LOCAL_RANK", "0")), None)
@@ -286,6 +342,9 @@ def main():
     ap.add_argument("--learned", default=DEFAULT_INDICATOR,
                     help="weights of the learned a-priori indicator ('none': without it)")
     ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--batch-problems", type=int, default=512,
+                    help="problems of the batched-ensemble leg (0: skip it)")
+    ap.add_argument("--batch-steps", type=int, default=100)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -428,6 +487,11 @@ def main():
     plain = time_form(dict(c, precision="fp64")) if (args.precision != "fp64" or learned) else None
     mixed = time_form(dict(c, precision="fp32")) if (args.precision == "fp32" and learned) else None
 
+    # ---- batched ensemble: independent four-quadrant Riemann problems ----
+    batched = None
+    if args.batch_problems > 0:
+        batched = batched_leg(args, local, dist, world)
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -464,6 +528,7 @@ def main():
             "e2e": e2e,
             "plain_fp64": plain,
             "mixed_without_indicator": mixed,
+            "batched": batched,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
