@@ -475,10 +475,12 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 }
 
 // resident blocks per SM the register allocation is sized for: 2 (128
-// registers a thread); 3 (85) for the FP32 form where that does not spill
-// (2D, p <= 3: its per-point slices take half the registers of FP64)
+// registers a thread); for the FP32 form in 2D, whose per-point slices take
+// half the registers of FP64, 3 (85) at p <= 2 and 4 (64) at p = 3, where
+// the extra resident warps outweigh a few spilled registers (measured on
+// B200: 159 us against 178 us per predictor pass at 256^2)
 template <typename R, int D, int P>
-constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? 3 : 2;
+constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? (P == 3 ? 4 : 3) : 2;
 
 // ---------------------------------------------------------------------------
 // Picard pass: interpolation to flux points, Euler fluxes, LLF at element
@@ -579,8 +581,12 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         }
         if (!kBulk && multi && t > 0) __syncthreads();
         // ---- phase A: flux-point fluxes of every direction ----
-        // one list: interfaces (the heavier items) first, then interior flux
-        // points; every item runs with a compile-time direction
+        // one list: interfaces (about three times the work of an interior
+        // point: two extrapolations and an LLF solve) first, then interior
+        // flux points; every item runs with a compile-time direction. When
+        // the interfaces fit in one pass of the block, each of the first NFT
+        // threads takes one interface and the remaining threads share the
+        // interior points, which evens out the work before the barrier.
         {
             constexpr int NINT = NE * (nf - 2) * NTP;
             constexpr int NF0 = (TX + 1) * (NE / TX) * NTP;
@@ -588,7 +594,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
             constexpr int NF2 = D == 3 ? (TZ + 1) * (NE / TZ) * NTP : 0;
             constexpr int NFT = NF0 + NF1 + NF2;
             constexpr int total = NFT + D * NINT;
-            for (int q = tid; q < total; q += kThreads) {
+            auto item = [&](int q) {
                 if (q < NF0) picard_face_item<R, D, P, TX, TY, TZ, 0>(G, M, Ss, FX, o, q);
                 else if (q < NF0 + NF1) picard_face_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, o, q - NF0);
                 else if (D == 3 && q < NFT) picard_face_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
@@ -598,6 +604,17 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                     else if (r < 2 * NINT) picard_interior_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, r - NINT);
                     else picard_interior_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, r - 2 * NINT);
                 }
+            };
+            constexpr int TI = kThreads - NFT;  // threads left for the interior points
+            // (measured on B200 at 2D p=3: faster for every FP32 pass and the
+            // FP64 flux pass, slower for the FP64 predictor and corrector)
+            constexpr bool kBalanced = sizeof(R) == 4 || MODE == kFlux;
+            if constexpr (kBalanced && NFT > 0 && TI >= kThreads / 4) {
+                if (tid < NFT) item(tid);
+                else
+                    for (int r = tid - NFT; r < D * NINT; r += TI) item(NFT + r);
+            } else {
+                for (int q = tid; q < total; q += kThreads) item(q);
             }
         }
         __syncthreads();
