@@ -482,6 +482,10 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 template <typename R, int D, int P>
 constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? (P == 3 ? 4 : 3) : 2;
 
+// flux-point buffers of a Picard pass (alternated between slices when 2)
+template <typename R>
+constexpr int kFxBuffers = sizeof(R) == 4 ? 2 : 1;
+
 // ---------------------------------------------------------------------------
 // Picard pass: interpolation to flux points, Euler fluxes, LLF at element
 // interfaces, flux divergence and the ADER predictor / corrector update,
@@ -506,8 +510,15 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R* smem = reinterpret_cast<R*>(smem_raw);
     R* Sbuf = smem;                     // 2 x [NS][SS >= V*NPT] (R buffer)
-    R* FX = Sbuf + 2 * NS * SS;         // [D][NE][V][FXS >= NFP]
-    R* TT = FX + D * NE * V * FXS;      // [NE][V][NFP] face-integral scratch (3D)
+    // [kFxBuffers][D][NE][V][FXS >= NFP]: with two buffers (FP32) the
+    // predictor and the corrector alternate them between slices, so a
+    // slice's flux points can be written while slow threads still read the
+    // previous slice's (no end-of-slice barrier); the flux pass uses the
+    // first only. FP64 keeps one buffer: its occupancy is bound by shared
+    // memory, and the larger footprint cost more than the barrier saved.
+    constexpr int NFX = kFxBuffers<R>;
+    R* FX0 = Sbuf + 2 * NS * SS;
+    R* TT = FX0 + NFX * D * NE * V * FXS;  // [NE][V][NFP] face-integral scratch (3D)
     __shared__ long long sl_elem[NS];
     __shared__ uint64_t bar[2];
 
@@ -574,6 +585,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         // ---- stage slice t (prefetch t+1 into the other buffer) ----
         const int b = multi ? (t & 1) : 0;
         R* Ss = Sbuf + b * NS * SS;
+        R* FX = FX0 + (NFX == 1 || MODE == kFlux ? 0 : (t & 1)) * (D * NE * V * FXS);
         if (multi && t + 1 < nt) issue(t + 1, b ^ 1);
         if (t == 0 || multi) {
             if (kBulk) mbar_wait_bounded(&bar[b], multi ? ((t >> 1) & 1) : 0, G.status);
@@ -748,8 +760,12 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                 }
             }
         }
-        __syncthreads();
+        // one FX buffer is reused by the next slice; the next slice's staging
+        // overwrites this slice's buffer, which the corrector's gravity
+        // source still reads; the flux pass reuses FX
+        if (NFX == 1 || MODE == kFlux || (MODE == kCorrect && G.grav)) __syncthreads();
     }
+    __syncthreads();
 
     if (MODE == kPredict) {
         // ---- ADER predictor (src/transforms.cpp:309-323) ----
@@ -894,7 +910,7 @@ constexpr size_t picard_smem_bytes() {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     size_t a = 2 * (size_t)TL::NS * PicardPad<D, P, R>::SS;
-    size_t b = (size_t)D * TL::NE * S::V * PicardPad<D, P, R>::FXS;
+    size_t b = (size_t)kFxBuffers<R> * D * TL::NE * S::V * PicardPad<D, P, R>::FXS;
     size_t c = (size_t)TL::NE * S::V * S::NFP;
     size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
     size_t total = a + b + c;

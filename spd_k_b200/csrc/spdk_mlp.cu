@@ -170,6 +170,110 @@ __global__ void __launch_bounds__(kThreadsM) k_mlp_forward(int n_in, const uint1
     }
 }
 
+// Inference: a persistent grid; each block keeps the parameters in shared
+// memory and walks tiles of 128 samples, each thread accumulating 4 hidden
+// units x 8 samples in registers (12 shared loads per 32 FMAs). The sums
+// run over k in the same order as forward_tile, so the probabilities are
+// the same as the training kernels'.
+constexpr int kSI = 128;  // samples per inference tile
+constexpr size_t kInferSmemMax = 200 * 1024;
+struct InferSmem {
+    int wbytes, xoff, h1, total;
+};
+__host__ __device__ inline InferSmem infer_smem(int n_in) {
+    const Layout L = layout(n_in);
+    InferSmem s;
+    s.wbytes = ((L.n * 2 + 15) / 16) * 16;
+    s.xoff = s.wbytes;
+    s.h1 = s.xoff + kSI * n_in * 4;
+    s.total = s.h1 + kSI * kH * 4;
+    return s;
+}
+
+__global__ void __launch_bounds__(kThreadsM) k_mlp_infer(int n_in, const uint16_t* __restrict__ wbf,
+                                                           const uint16_t* __restrict__ x, long long batch,
+                                                           float* __restrict__ p, uint8_t* __restrict__ flags,
+                                                           float thr) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const Layout L = layout(n_in);
+    const InferSmem S = infer_smem(n_in);
+    load_params(L, sm, wbf);
+    const uint16_t* W = reinterpret_cast<const uint16_t*>(sm);
+    float* X = reinterpret_cast<float*>(sm + S.xoff);
+    float* H1 = reinterpret_cast<float*>(sm + S.h1);
+    const int j0 = threadIdx.x % 16, g = threadIdx.x / 16;  // units j0 + 16u, samples g + 16r
+    const long long tiles = (batch + kSI - 1) / kSI;
+    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const long long s0 = tile * kSI;
+        for (int q = threadIdx.x; q < kSI * n_in; q += blockDim.x) {
+            const int s = q / n_in, k = q % n_in;
+            X[q] = (s0 + s < batch) ? bf(x[(s0 + s) * n_in + k]) : 0.0f;
+        }
+        __syncthreads();
+        // two hidden layers: in [kSI][nk] -> gelu(in W + b); the first goes
+        // to H1, the second straight into the output dot product
+        float zp[8];
+        for (int layer = 0; layer < 2; layer++) {
+            const float* in = layer == 0 ? X : H1;
+            const int nk = layer == 0 ? n_in : kH;
+            const int oW = layer == 0 ? L.oW1 : L.oW2, ob = layer == 0 ? L.ob1 : L.ob2;
+            float acc[8][4];
+#pragma unroll
+            for (int r = 0; r < 8; r++)
+#pragma unroll
+                for (int u = 0; u < 4; u++) acc[r][u] = 0.0f;
+            for (int k = 0; k < nk; k++) {
+                float w[4], xv[8];
+#pragma unroll
+                for (int u = 0; u < 4; u++) w[u] = bf(W[oW + k * kH + j0 + 16 * u]);
+#pragma unroll
+                for (int r = 0; r < 8; r++) xv[r] = in[(g + 16 * r) * nk + k];
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+#pragma unroll
+                    for (int u = 0; u < 4; u++) acc[r][u] += xv[r] * w[u];
+            }
+            if (layer == 0) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const float b = bf(W[ob + j0 + 16 * u]);
+#pragma unroll
+                    for (int r = 0; r < 8; r++) H1[(g + 16 * r) * kH + j0 + 16 * u] = gelu(acc[r][u] + b);
+                }
+                __syncthreads();
+            } else {
+                // this thread's 4 units of w3 . H2 for its 8 samples, then the
+                // 16 threads of a sample group (consecutive lanes) add up
+#pragma unroll
+                for (int r = 0; r < 8; r++) zp[r] = 0.0f;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const float b = bf(W[ob + j0 + 16 * u]), w3 = bf(W[L.ow3 + j0 + 16 * u]);
+#pragma unroll
+                    for (int r = 0; r < 8; r++) zp[r] += gelu(acc[r][u] + b) * w3;
+                }
+#pragma unroll
+                for (int r = 0; r < 8; r++)
+#pragma unroll
+                    for (int off = 8; off > 0; off >>= 1) zp[r] += __shfl_xor_sync(0xffffffffu, zp[r], off);
+            }
+        }
+        if (j0 == 0) {
+            const float b3 = bf(W[L.ob3]);
+#pragma unroll
+            for (int r = 0; r < 8; r++) {
+                const long long s = s0 + g + 16 * r;
+                if (s < batch) {
+                    const float pr = 1.0f / (1.0f + expf(-(zp[r] + b3)));
+                    if (p) p[s] = pr;
+                    if (flags) flags[s] = pr > thr ? 1 : 0;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // per block: sum_s w_s BCE_s, sum_s w_s and the unnormalised gradient
 // sum_s w_s dBCE_s/dtheta into part[block][0 .. n+1]
 __global__ void __launch_bounds__(kThreadsM) k_mlp_grad(int n_in, const uint16_t* __restrict__ wbf,
@@ -321,18 +425,29 @@ __device__ __forceinline__ void rho_p_point(const R* u, int V, int NPT, int pt, 
     *p = ((double)u[(V - 1) * NPT + pt] - 0.5 * m2 / r) * (gm - 1.0);
 }
 
+// per element: mean density and mean pressure over the solution points,
+// summed in point order; one thread per (element, point), 256 threads =
+// 256 / NPT elements (or one element and several rounds)
 template <typename R>
-__global__ void k_elem_means(const R* __restrict__ u, int V, int NPT, long long E, double gm, float2* __restrict__ mean) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E; e += (long long)gridDim.x * blockDim.x) {
-        const R* ue = u + e * V * NPT;
+__global__ void k_elem_means(const R* __restrict__ u, int V, int NPT, long long E, double gm,
+                             float2* __restrict__ mean) {
+    extern __shared__ double2 rp[];  // [elements of the block][NPT]
+    const int per = NPT >= (int)blockDim.x ? 1 : (int)blockDim.x / NPT;
+    const long long e0 = (long long)blockIdx.x * per;
+    for (int q = threadIdx.x; q < per * NPT; q += blockDim.x) {
+        const int el = q / NPT, pt = q % NPT;
+        double r = 1.0, p = 1.0;
+        if (e0 + el < E) rho_p_point(u + (e0 + el) * V * NPT, V, NPT, pt, gm, &r, &p);
+        rp[q] = make_double2(r, p);
+    }
+    __syncthreads();
+    if (threadIdx.x < per && e0 + threadIdx.x < E) {
         double sr = 0, sp = 0;
         for (int pt = 0; pt < NPT; pt++) {
-            double r, p;
-            rho_p_point(ue, V, NPT, pt, gm, &r, &p);
-            sr += r;
-            sp += p;
+            sr += rp[threadIdx.x * NPT + pt].x;
+            sp += rp[threadIdx.x * NPT + pt].y;
         }
-        mean[e] = make_float2((float)(sr / NPT), (float)(sp / NPT));
+        mean[e0 + threadIdx.x] = make_float2((float)(sr / NPT), (float)(sp / NPT));
     }
 }
 
@@ -341,40 +456,48 @@ __device__ __forceinline__ float safe_ratio(double a, double b) {
     return isfinite(r) ? (float)r : 0.0f;
 }
 
+// feature rows: the nodal part one thread per (element, point), the
+// neighbour part one thread per (element, direction)
 template <typename R>
 __global__ void k_features(const R* __restrict__ u, const float2* __restrict__ mean, int D, int V, int NPT, int N0,
                            int N1, int N2, int bc0, int bc1, int bc2, long long E, double gm, int n_in,
                            uint16_t* __restrict__ x) {
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < E; e += (long long)gridDim.x * blockDim.x) {
-        const R* ue = u + e * V * NPT;
-        uint16_t* row = x + e * n_in;
+    const int per = NPT >= (int)blockDim.x ? 1 : (int)blockDim.x / NPT;
+    const long long e0 = (long long)blockIdx.x * per;
+    for (int q = threadIdx.x; q < per * NPT; q += blockDim.x) {
+        const int el = q / NPT, pt = q % NPT;
+        const long long e = e0 + el;
+        if (e >= E) continue;
+        double r, p;
+        rho_p_point(u + e * V * NPT, V, NPT, pt, gm, &r, &p);
         const float2 me = mean[e];
-        for (int pt = 0; pt < NPT; pt++) {
-            double r, p;
-            rho_p_point(ue, V, NPT, pt, gm, &r, &p);
-            row[pt] = to_bf(safe_ratio(r, me.x));
-            row[NPT + pt] = to_bf(safe_ratio(p, me.y));
-        }
+        x[e * n_in + pt] = to_bf(safe_ratio(r, me.x));
+        x[e * n_in + NPT + pt] = to_bf(safe_ratio(p, me.y));
+    }
+    for (int q = threadIdx.x; q < per * D; q += blockDim.x) {
+        const long long e = e0 + q / D;
+        const int d = q % D;
+        if (e >= E) continue;
+        const float2 me = mean[e];
         const int N[3] = {N0, N1, N2}, bc[3] = {bc0, bc1, bc2};
-        int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
-        for (int d = 0; d < D; d++) {
-            float2 nb[2];
-            for (int sd = 0; sd < 2; sd++) {
-                int cc[3] = {c[0], c[1], c[2]};
-                cc[d] += sd ? 1 : -1;
-                if (cc[d] < 0 || cc[d] >= N[d]) {
-                    if (bc[d] == SPDK_BC_PERIODIC) cc[d] = cc[d] < 0 ? cc[d] + N[d] : cc[d] - N[d];
-                    else cc[d] = c[d];  // outside the domain: the element itself
-                }
-                nb[sd] = mean[((long long)cc[2] * N1 + cc[1]) * N0 + cc[0]];
+        const int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
+        float2 nb[2];
+        for (int sd = 0; sd < 2; sd++) {
+            int cc[3] = {c[0], c[1], c[2]};
+            cc[d] += sd ? 1 : -1;
+            if (cc[d] < 0 || cc[d] >= N[d]) {
+                if (bc[d] == SPDK_BC_PERIODIC) cc[d] = cc[d] < 0 ? cc[d] + N[d] : cc[d] - N[d];
+                else cc[d] = c[d];  // outside the domain: the element itself
             }
-            const float r0 = safe_ratio(nb[0].x, me.x), r1 = safe_ratio(nb[1].x, me.x);
-            const float p0 = safe_ratio(nb[0].y, me.y), p1 = safe_ratio(nb[1].y, me.y);
-            row[2 * NPT + 4 * d + 0] = to_bf(fminf(r0, r1));
-            row[2 * NPT + 4 * d + 1] = to_bf(fmaxf(r0, r1));
-            row[2 * NPT + 4 * d + 2] = to_bf(fminf(p0, p1));
-            row[2 * NPT + 4 * d + 3] = to_bf(fmaxf(p0, p1));
+            nb[sd] = mean[((long long)cc[2] * N1 + cc[1]) * N0 + cc[0]];
         }
+        const float r0 = safe_ratio(nb[0].x, me.x), r1 = safe_ratio(nb[1].x, me.x);
+        const float p0 = safe_ratio(nb[0].y, me.y), p1 = safe_ratio(nb[1].y, me.y);
+        uint16_t* row = x + e * n_in + 2 * NPT + 4 * d;
+        row[0] = to_bf(fminf(r0, r1));
+        row[1] = to_bf(fmaxf(r0, r1));
+        row[2] = to_bf(fminf(p0, p1));
+        row[3] = to_bf(fmaxf(p0, p1));
     }
 }
 
@@ -392,15 +515,22 @@ struct spdk_mlp {
     uint16_t* wbf = nullptr;
     int part_blocks = 0;
     long long step = 0;
-    size_t smem = 0;
+    size_t smem = 0, infer_smem = 0;
 };
 
 namespace spdk {
 
 int mlp_infer_flags(spdk_mlp* m, const uint16_t* x, long long batch, float* p, uint8_t* flags, float thr,
                     cudaStream_t s) {
-    const unsigned blocks = (unsigned)((batch + kSB - 1) / kSB);
-    k_mlp_forward<<<blocks, kThreadsM, m->smem, s>>>(m->n_in, m->wbf, x, (int)batch, p, flags, thr);
+    if (m->infer_smem <= kInferSmemMax) {
+        const long long tiles = (batch + kSI - 1) / kSI;
+        const unsigned blocks = (unsigned)(tiles < 148LL * 2 ? tiles : 148LL * 2);
+        k_mlp_infer<<<blocks, kThreadsM, m->infer_smem, s>>>(m->n_in, m->wbf, x, batch, p, flags, thr);
+    } else {
+        // wide inputs (3D, high order): the 32-sample tiles of the training kernels
+        const unsigned blocks = (unsigned)((batch + kSB - 1) / kSB);
+        k_mlp_forward<<<blocks, kThreadsM, m->smem, s>>>(m->n_in, m->wbf, x, (int)batch, p, flags, thr);
+    }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("indicator: ") + cudaGetErrorString(e));
 }
@@ -408,15 +538,18 @@ int mlp_infer_flags(spdk_mlp* m, const uint16_t* x, long long batch, float* p, u
 int feature_rows(const void* u, bool fp32, int D, int p, const int N[3], const int bc[3], double gm, long long E,
                  float2* means, uint16_t* x, cudaStream_t s) {
     const int n = p + 1, NPT = D == 2 ? n * n : n * n * n, V = D + 2, n_in = 2 * NPT + 4 * D;
-    const unsigned g = grid_for(E, 128);
+    const int threads = 256;
+    const int per = NPT >= threads ? 1 : threads / NPT;
+    const unsigned g = (unsigned)((E + per - 1) / per);
+    const size_t sm = (size_t)per * NPT * sizeof(double2);
     if (fp32) {
-        k_elem_means<float><<<g, 128, 0, s>>>((const float*)u, V, NPT, E, gm, means);
-        k_features<float><<<g, 128, 0, s>>>((const float*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1], bc[2],
-                                             E, gm, n_in, x);
+        k_elem_means<float><<<g, threads, sm, s>>>((const float*)u, V, NPT, E, gm, means);
+        k_features<float><<<g, threads, 0, s>>>((const float*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1],
+                                                 bc[2], E, gm, n_in, x);
     } else {
-        k_elem_means<double><<<g, 128, 0, s>>>((const double*)u, V, NPT, E, gm, means);
-        k_features<double><<<g, 128, 0, s>>>((const double*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1],
-                                              bc[2], E, gm, n_in, x);
+        k_elem_means<double><<<g, threads, sm, s>>>((const double*)u, V, NPT, E, gm, means);
+        k_features<double><<<g, threads, 0, s>>>((const double*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1],
+                                                  bc[2], E, gm, n_in, x);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("features: ") + cudaGetErrorString(e));
@@ -438,6 +571,7 @@ int spdk_mlp_create(int n_in, int hidden, unsigned long long seed, spdk_mlp** ou
     const Layout L = layout(n_in);
     m->n = L.n;
     m->smem = (size_t)smem_layout(n_in).total;
+    m->infer_smem = (size_t)infer_smem(n_in).total;
     // seeded Glorot-uniform weights (SplitMix64 stream), zero biases
     std::vector<float> w(L.n, 0.0f);
     uint64_t st = seed;
@@ -469,7 +603,10 @@ int spdk_mlp_create(int n_in, int hidden, unsigned long long seed, spdk_mlp** ou
         k_to_bf16<<<grid_for(L.n, 256), 256>>>(m->w, m->wbf, L.n);
         if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem) !=
                 cudaSuccess ||
-            cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem) != cudaSuccess)
+            cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem) != cudaSuccess ||
+            (m->infer_smem <= kInferSmemMax &&
+             cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->infer_smem) !=
+                 cudaSuccess))
             rc = fail(SPDK_E_CUDA, "mlp shared memory request");
         if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = fail(SPDK_E_CUDA, "mlp init");
     }
