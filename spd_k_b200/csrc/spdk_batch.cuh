@@ -14,10 +14,6 @@ struct DetectArgs {
     const double2* rpn;
     uint8_t* T;
 };
-struct ThetaArgs {
-    const uint8_t* T;
-    uint8_t* theta;
-};
 struct DtArgs {
     double* dt;
     unsigned long long* dtmin;
@@ -65,21 +61,14 @@ __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>)
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) detect_batched(const BatchItem<DetectArgs>* __restrict__ items, int n) {
+__global__ void __launch_bounds__(kThreads, kDetectBlocksPerSM<D>) detect_batched(const BatchItem<DetectArgs>* __restrict__ items, int n) {
     long long b;
     const BatchItem<DetectArgs>& it = batch_item(items, n, &b);
     fv_detect_kernel_body<R, D, P, TX, TY, TZ>(it.G, it.A.rpo, it.A.rpn, it.A.T, nullptr, b);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) theta_batched(const BatchItem<ThetaArgs>* __restrict__ items, int n) {
-    long long b;
-    const BatchItem<ThetaArgs>& it = batch_item(items, n, &b);
-    fv_theta_kernel_body<R, D, P, TX, TY, TZ>(it.G, it.A.T, it.A.theta, b);
-}
-
-template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D>)
     update_batched(const BatchItem<FallbackArgsT<R>>* __restrict__ items, int n, DevMatsT<R> M) {
     long long b;
     const BatchItem<FallbackArgsT<R>>& it = batch_item(items, n, &b);
@@ -95,7 +84,6 @@ struct BatchSetT {
     void (*correct)(const BatchItem<PicardArgsT<R>>*, int, DevMatsT<R>) = nullptr;
     void (*flux)(const BatchItem<PicardArgsT<R>>*, int, DevMatsT<R>) = nullptr;
     void (*detect)(const BatchItem<DetectArgs>*, int) = nullptr;
-    void (*theta)(const BatchItem<ThetaArgs>*, int) = nullptr;
     void (*update)(const BatchItem<FallbackArgsT<R>>*, int, DevMatsT<R>) = nullptr;
     size_t picard_smem = 0, update_smem = 0;
     int tile[3] = {1, 1, 1};
@@ -108,7 +96,6 @@ BatchSetT<R> make_batch_set() {
     k.correct = picard_batched<R, 2, P, TX, TY, 1, kCorrect>;
     k.flux = picard_batched<R, 2, P, TX, TY, 1, kFlux>;
     k.detect = detect_batched<R, 2, P, TX, TY, 1>;
-    k.theta = theta_batched<R, 2, P, TX, TY, 1>;
     k.update = update_batched<R, 2, P, TX, TY, 1>;
     k.picard_smem = picard_smem_bytes<R, 2, P, TX, TY, 1>();
     k.update_smem = UpdateSmem<R, 2, P, TX, TY, 1>::bytes;

@@ -34,7 +34,7 @@ __global__ void dt_batched(const DtArgs* __restrict__ a, int n) {
 
 namespace {
 
-enum { kPassPredict, kPassCorrect, kPassFlux, kPassDetect, kPassTheta, kPassUpdate };
+enum { kPassPredict, kPassCorrect, kPassFlux, kPassDetect, kPassUpdate };
 
 struct Pass {
     int kind;
@@ -172,7 +172,6 @@ int plan_group(spdk_batch* b, Group& g) {
     }
     for (int t = 0; t < nt && !rc; t++) {
         std::vector<BatchItem<DetectArgs>> det(n);
-        std::vector<BatchItem<ThetaArgs>> th(n);
         std::vector<BatchItem<FallbackArgsT<R>>> up(n);
         for (int q = 0; q < n; q++) {
             spdk_hydro* h = b->probs[g.members[q]];
@@ -180,9 +179,6 @@ int plan_group(spdk_batch* b, Group& g) {
             det[q].G = bq.G;
             det[q].first = bq.first;
             det[q].A = DetectArgs{h->rpo, h->rpn, h->trouble};
-            th[q].G = bq.G;
-            th[q].first = bq.first;
-            th[q].A = ThetaArgs{h->trouble, h->theta};
             up[q].G = bq.G;
             up[q].first = bq.first;
             FallbackArgsT<R>& F = up[q].A;
@@ -209,7 +205,6 @@ int plan_group(spdk_batch* b, Group& g) {
             F.dt = h->dt;
         }
         rc = upload_pass(g, kPassDetect, blocks, det);
-        if (!rc) rc = upload_pass(g, kPassTheta, blocks, th);
         if (!rc) rc = upload_pass(g, kPassUpdate, blocks, up);
     }
     return rc;
@@ -248,19 +243,16 @@ int launch_group_t(spdk_batch* b, const Group& g, cudaStream_t st) {
         b->prec == SPDK_PRECISION_FP32 ? (const void*)&h0->dm32 : (const void*)&h0->dm64);
     using PI = BatchItem<PicardArgsT<R>>;
     using DI = BatchItem<DetectArgs>;
-    using TI = BatchItem<ThetaArgs>;
     using UI = BatchItem<FallbackArgsT<R>>;
     for (const Pass& p : g.passes) {
         const PI* pi = static_cast<const PI*>(p.items);
         const DI* di = static_cast<const DI*>(p.items);
-        const TI* ti = static_cast<const TI*>(p.items);
         const UI* ui = static_cast<const UI*>(p.items);
         switch (p.kind) {
         case kPassPredict: k.predict<<<p.blocks, kThreads, k.picard_smem, st>>>(pi, p.n, dm); break;
         case kPassCorrect: k.correct<<<p.blocks, kThreads, k.picard_smem, st>>>(pi, p.n, dm); break;
         case kPassFlux: k.flux<<<p.blocks, kThreads, k.picard_smem, st>>>(pi, p.n, dm); break;
         case kPassDetect: k.detect<<<p.blocks, kThreads, 0, st>>>(di, p.n); break;
-        case kPassTheta: k.theta<<<p.blocks, kThreads, 0, st>>>(ti, p.n); break;
         case kPassUpdate: k.update<<<p.blocks, kThreads, k.update_smem, st>>>(ui, p.n, dm); break;
         }
     }

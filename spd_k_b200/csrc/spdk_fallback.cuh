@@ -37,6 +37,12 @@ struct FallbackArgsT {
     unsigned long long* dtmin;
     const double* dt;
     int* any_trouble;       // diagnostic counter of troubled sub-cells (nullable)
+    // learned indicator (nullable): after the final stage, the element means
+    // of (rho, p) and the nodal part of each feature row (row length n_in)
+    // of the new state, for the next step's a-priori flags
+    uint16_t* feat;
+    float2* means;
+    int n_in;
 };
 using FallbackArgs = FallbackArgsT<double>;
 
@@ -79,44 +85,112 @@ __device__ __forceinline__ double rp_var(const double2 v, int k) { return k == 0
 // it everywhere. W_old (rho, p) of the tile + 1 halo is staged in shared
 // memory for the NAD box.
 // ---------------------------------------------------------------------------
+// FV axes of the smooth-extrema indicator: active cells and the ghost-framed
+// centre / face coordinates of each direction
+struct SedGeom {
+    int nd[3];
+    const double* C[3];
+    const double* Fc[3];
+};
+
 template <int D, int P>
-__device__ __forceinline__ double sed_component(const DevGrid& G, const double2* __restrict__ rpn, const int a[3],
-                                                int d, int k) {
-    constexpr int n = P + 1;
-    const int nd = G.N[d] * n;
-    const double* C = G.fvc[d];
-    const double* Fc = G.fvf[d];
+__device__ __forceinline__ SedGeom sed_geom(const DevGrid& G) {
+    SedGeom S;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        S.nd[d] = G.N[d] * (P + 1);
+        S.C[d] = G.fvc[d];
+        S.Fc[d] = G.fvf[d];
+    }
+    return S;
+}
+
+// rpv(b, k): variable k (rho, p) of the candidate at FV coordinate b, which
+// lies at most two cells outside the active cells.
+// The smooth-extrema alpha of position a in direction d (0 outside the
+// active cells, where the reference never computes it).
+template <typename RPV>
+__device__ __forceinline__ double sed_al(const SedGeom& S, const RPV& rpv, const int a[3], int d, int k) {
+    const int ad = a[d];
+    if (ad < 0 || ad >= S.nd[d]) return 0.0;
+    const double* C = S.C[d];
+    const double* Fc = S.Fc[d];
+    int b[3] = {a[0], a[1], a[2]};
+    double Wv[5];
+#pragma unroll
+    for (int off = -2; off <= 2; off++) {
+        b[d] = ad + off;
+        Wv[off + 2] = rpv(b, k);
+    }
+    const int l = ad + 2;
+    const double h = (C[l + 1] - C[l - 1]);
+    const double hp = (C[l + 2] - C[l]);
+    const double hm = (C[l] - C[l - 2]);
+    const double u = Wv[2];
+    const double du = (Wv[3] - Wv[1]) / h;
+    const double dup = (Wv[4] - u) / hp;
+    const double dum = (u - Wv[0]) / hm;
+    const double d2u = (dup - dum) / (C[l + 1] - C[l - 1]);
+    const double dv = 0.5 * d2u * (Fc[l + 1] - Fc[l]);
+    return sed_alpha(dv, dum, du, dup);
+}
+
+// min of the alphas of the cell and its two neighbours in direction d
+template <typename RPV>
+__device__ __forceinline__ double sed_component(const SedGeom& S, const RPV& rpv, const int a[3], int d, int k) {
     double al[3];
-    bool fl[3];
 #pragma unroll
     for (int s = -1; s <= 1; s++) {
-        const int ad = a[d] + s;
-        if (ad < 0 || ad >= nd) { al[s + 1] = 0.0; continue; }  // never computed outside the active cells
         int b[3] = {a[0], a[1], a[2]};
-        double Wv[5];
-#pragma unroll
-        for (int off = -2; off <= 2; off++) {
-            b[d] = ad + off;
-            Wv[off + 2] = rp_var(rpn[cell_image<D, P>(G, b, fl)], k);
-        }
-        const int l = ad + 2;
-        const double h = (C[l + 1] - C[l - 1]);
-        const double hp = (C[l + 2] - C[l]);
-        const double hm = (C[l] - C[l - 2]);
-        const double u = Wv[2];
-        const double du = (Wv[3] - Wv[1]) / h;
-        const double dup = (Wv[4] - u) / hp;
-        const double dum = (u - Wv[0]) / hm;
-        const double d2u = (dup - dum) / (C[l + 1] - C[l - 1]);
-        const double dv = 0.5 * d2u * (Fc[l + 1] - Fc[l]);
-        al[s + 1] = sed_alpha(dv, dum, du, dup);
+        b[d] += s;
+        al[s + 1] = sed_al(S, rpv, b, d, k);
     }
     return smin(smin(al[0], al[1]), al[2]);
+}
+
+// min over the directions of the SED alpha of 2D cell (ax, ay), variable k,
+// from candidates staged on the tile + 3 halo (Rn, row length E3x, origin
+// ox - 3, oy - 3). Not inlined: the rare flagged cells pay for its registers
+// in its own frame, and the NAD pass of every cell keeps to its cap.
+static __device__ __noinline__ double sed_alpha_staged_2d(const SedGeom S, const double2* Rn, int E3x, int ox, int oy,
+                                                         int ax, int ay, int k) {
+    auto staged = [&](const int b[3], int kk) { return rp_var(Rn[(b[0] - ox + 3) + E3x * (b[1] - oy + 3)], kk); };
+    const int a[3] = {ax, ay, 0};
+    const double m0 = sed_component(S, staged, a, 0, k);
+    return smin(m0, sed_component(S, staged, a, 1, k));
+}
+
+// every alpha of the 2D tile + 1 halo (E1x x E1y positions from ox - 1,
+// oy - 1) of the variables in kmask, by the whole block: Al[(k * 2 + d) *
+// E1x * E1y + position]; for blocks with many flagged cells, whose
+// neighbours would otherwise evaluate the same positions again
+static __device__ __noinline__ void sed_al_tile_2d(const SedGeom S, const double2* Rn, int E3x, int E1x, int E1y,
+                                                   int ox, int oy, unsigned kmask, double* Al) {
+    auto staged = [&](const int b[3], int kk) { return rp_var(Rn[(b[0] - ox + 3) + E3x * (b[1] - oy + 3)], kk); };
+    const int np = E1x * E1y;
+    for (int w = threadIdx.x; w < 4 * np; w += blockDim.x) {
+        const int pos = w % np, kd = w / np, k = kd >> 1, d = kd & 1;
+        if (!((kmask >> k) & 1u)) continue;
+        const int a[3] = {ox - 1 + pos % E1x, oy - 1 + pos / E1x, 0};
+        Al[w] = sed_al(S, staged, a, d, k);
+    }
 }
 
 // R names the form (double: plain, float: precision) that launches the
 // kernel; the detector computes in FP64 in both, and a separate
 // instantiation per form keeps each form's compile flags on its own copy.
+//
+// Each thread loads its cells' candidates before it stages the tile's W_old,
+// so a block waits for one memory round trip, not two. In 2D the kernel is
+// compiled for 4 resident blocks (64 registers, the NAD pass unspilled;
+// measured on B200: 38.6 us against 43.2 us at 6 blocks with spills); in
+// 3D, whose SED reads global memory, without a cap.
+template <int D>
+constexpr int kDetectBlocksPerSM = D == 2 ? 4 : 1;
+// flagged threads of a block above which it evaluates every alpha of its
+// tile once instead of each flagged cell evaluating its own six
+constexpr int kSedTileThreshold = 24;
+
 template <typename R, int D, int P, int TX, int TY, int TZ>
 __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
@@ -125,7 +199,13 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
     constexpr int NPT = Shape<D, P>::NPT;
     constexpr int Bx = TX * n, By = TY * n, Bz = D == 3 ? TZ * n : 1;
     constexpr int E1x = Bx + 2, E1y = By + 2, E1z = D == 3 ? Bz + 2 : 1;
+    constexpr int NC = Bx * By * Bz;
+    constexpr int CPT = (NC + kThreads - 1) / kThreads;  // cells per thread
+    static_assert(CPT <= 16, "NAD flag bits");
+    constexpr int E3x = Bx + 6, E3y = By + 6;
     __shared__ double2 Ro[E1x * E1y * E1z];
+    __shared__ double2 Rn[D == 2 ? E3x * E3y : 1];
+    __shared__ double Al[D == 2 ? 4 * E1x * E1y : 1];
     const int dz = D == 3 ? 1 : 0;
     int o[3];
     {
@@ -137,22 +217,32 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
         b /= ty;
         o[2] = D == 3 ? b * Bz : 0;
     }
+    double2 here_new[CPT];
+#pragma unroll
+    for (int r = 0; r < CPT; r++) {
+        const int q = threadIdx.x + r * kThreads;
+        if (NC % kThreads == 0 || q < NC) {
+            int a[3] = {o[0] + q % Bx, o[1] + (q / Bx) % By, o[2] + q / (Bx * By)};
+            here_new[r] = rpn[cell_id<D, P>(G, a)];
+        }
+    }
     for (int q = threadIdx.x; q < E1x * E1y * E1z; q += blockDim.x) {
         int a[3] = {o[0] - 1 + q % E1x, o[1] - 1 + (q / E1x) % E1y, o[2] - dz + q / (E1x * E1y)};
         bool fl[3];
         Ro[q] = rpo[cell_image<D, P>(G, a, fl)];
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < Bx * By * Bz; q += blockDim.x) {
+    // NAD flags of this thread's cells: bit 2r + k for variable k of cell r
+    unsigned nad = 0;
+#pragma unroll
+    for (int r = 0; r < CPT; r++) {
+        const int q = threadIdx.x + r * kThreads;
+        if (NC % kThreads != 0 && q >= NC) break;
         const int x = q % Bx, y = (q / Bx) % By, z = q / (Bx * By);
-        int a[3] = {o[0] + x, o[1] + y, o[2] + z};
-        const long long cid = cell_id<D, P>(G, a);
-        const double2 here_new = rpn[cid];
         const int sc = (x + 1) + E1x * ((y + 1) + E1y * (z + dz));
-        double flag[2];
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-            const double un = rp_var(here_new, k);
+            const double un = rp_var(here_new[r], k);
             double mx = rp_var(Ro[sc], k), mn = mx;
             if (G.nad_moore) {
                 for (int ok = -dz; ok <= dz; ok++)
@@ -182,126 +272,194 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
                 mn -= fabs(mn) * G.nad_tol;
                 mx += fabs(mx) * G.nad_tol;
             }
-            flag[k] = (un > mx || un < mn) ? 1.0 : 0.0;
+            if (un > mx || un < mn) nad |= 1u << (2 * r + k);
         }
-        if (G.use_sed) {
+    }
+    // SED relaxation of the NAD flags (it can only clear one). In 2D the
+    // block stages the candidates of the tile + 3 halo once when any of its
+    // cells needs it, so a flagged cell reads its stencils from shared
+    // memory instead of a chain of global loads.
+    const int nflag = G.use_sed ? __syncthreads_count(nad != 0) : 0;
+    if (nflag) {
+        if (D == 2) {
+            for (int q = threadIdx.x; q < E3x * E3y; q += blockDim.x) {
+                int a[3] = {o[0] - 3 + q % E3x, o[1] - 3 + q / E3x, 0};
+                // three cells outside a non-periodic boundary: never read
+                const bool outside = (G.bc[0] != kPeriodic && (a[0] < -2 || a[0] >= G.N[0] * n + 2)) ||
+                                     (G.bc[1] != kPeriodic && (a[1] < -2 || a[1] >= G.N[1] * n + 2));
+                bool fl[3];
+                Rn[q] = outside ? make_double2(0.0, 0.0) : rpn[cell_image<D, P>(G, a, fl)];
+            }
+            __syncthreads();
+        }
+        const SedGeom SG = sed_geom<D, P>(G);
+        auto global = [&](const int b[3], int k) {
+            bool fl[3];
+            return rp_var(rpn[cell_image<D, P>(G, b, fl)], k);
+        };
+        const bool tile = D == 2 && nflag > kSedTileThreshold;
+        if (tile) {
+            const unsigned kmask = (__syncthreads_or(nad & 0x55555555u) ? 1u : 0u) |
+                                   (__syncthreads_or(nad & 0xAAAAAAAAu) ? 2u : 0u);
+            sed_al_tile_2d(SG, Rn, E3x, E1x, E1y, o[0], o[1], kmask, Al);
+            __syncthreads();
+        }
+#pragma unroll
+        for (int r = 0; r < CPT; r++) {
+            if (!(nad & (3u << (2 * r)))) continue;
+            const int q = threadIdx.x + r * kThreads;
+            int a[3] = {o[0] + q % Bx, o[1] + (q / Bx) % By, o[2] + q / (Bx * By)};
 #pragma unroll
             for (int k = 0; k < 2; k++) {
-                if (flag[k] == 0.0) continue;  // relaxation cannot raise a flag
+                if (!(nad & (1u << (2 * r + k)))) continue;
                 double alpha = 1;
+                if (tile) {
+                    // the alphas of the cell and its neighbours, in the
+                    // order sed_component takes them
+                    const int x = a[0] - o[0] + 1, y = a[1] - o[1] + 1;
+                    const double* A0 = Al + (k * 2 + 0) * E1x * E1y;
+                    const double* A1 = Al + (k * 2 + 1) * E1x * E1y;
+                    const double m0 = smin(smin(A0[(x - 1) + E1x * y], A0[x + E1x * y]), A0[(x + 1) + E1x * y]);
+                    const double m1 = smin(smin(A1[x + E1x * (y - 1)], A1[x + E1x * y]), A1[x + E1x * (y + 1)]);
+                    alpha = smin(m0, m1);
+                } else if (D == 2) {
+                    alpha = sed_alpha_staged_2d(SG, Rn, E3x, o[0], o[1], a[0], a[1], k);
+                } else {
 #pragma unroll
-                for (int d = 0; d < D; d++) {
-                    const double m3 = sed_component<D, P>(G, rpn, a, d, k);
-                    alpha = d == 0 ? m3 : smin(alpha, m3);
+                    for (int d = 0; d < D; d++) {
+                        const double m3 = sed_component(SG, global, a, d, k);
+                        alpha = d == 0 ? m3 : smin(alpha, m3);
+                    }
                 }
-                flag[k] = alpha < 1 ? flag[k] : 0;
+                if (!(alpha < 1)) nad &= ~(1u << (2 * r + k));
             }
         }
-        double tr = 0;
-        tr = smax(tr, flag[0]);
-        tr = smax(tr, flag[1]);
-        const double rho = here_new.x, p = here_new.y;
-        if (rho < kRhoMin || rho > kRhoMax) tr = 1;
-        if (p < kPMin || p > kPMax) tr = 1;
+    }
+#pragma unroll
+    for (int r = 0; r < CPT; r++) {
+        const int q = threadIdx.x + r * kThreads;
+        if (NC % kThreads != 0 && q >= NC) break;
+        int a[3] = {o[0] + q % Bx, o[1] + (q / Bx) % By, o[2] + q / (Bx * By)};
+        const long long cid = cell_id<D, P>(G, a);
+        bool tr = (nad >> (2 * r)) & 3u;
+        const double rho = here_new[r].x, p = here_new[r].y;
+        if (rho < kRhoMin || rho > kRhoMax) tr = true;
+        if (p < kPMin || p > kPMax) tr = true;
         const long long el = cid / NPT;
-        if (G.elem_trouble && tr > 0) G.elem_trouble[el] = 1;  // a-posteriori label
-        if (G.elem_pred && G.elem_pred[el]) tr = 1;            // a-priori prediction
-        T[cid] = tr > 0 ? 1 : 0;
-        if (any_trouble && tr > 0) atomicAdd(any_trouble, 1);
+        if (G.elem_trouble && tr) G.elem_trouble[el] = 1;  // a-posteriori label
+        if (G.elem_pred && G.elem_pred[el]) tr = true;     // a-priori prediction
+        T[cid] = tr ? 1 : 0;
+        if (any_trouble && tr) atomicAdd(any_trouble, 1);
     }
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
+__global__ void __launch_bounds__(kThreads, kDetectBlocksPerSM<D>) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
                                                             uint8_t* __restrict__ T, int* any_trouble) {
     fv_detect_kernel_body<R, D, P, TX, TY, TZ>(G, rpo, rpn, T, any_trouble, blockIdx.x);
 }
 
-// cell box of an element tile with a halo of g cells per active side
-template <int D, int P, int TX, int TY, int TZ>
-struct CellBox {
-    static constexpr int n = P + 1;
-    __device__ static int ext(int d, int g) {
-        return d >= D ? 1 : (d == 0 ? TX : (d == 1 ? TY : TZ)) * n + 2 * g;
-    }
-};
-
 // ---------------------------------------------------------------------------
 // theta = max over the Moore box of w(#offsets) * trouble, plus the 0.25 ring
-// (src/trouble_detection.cpp:191-242); theta_from_troubles without blending
+// (src/trouble_detection.cpp:191-242; theta_from_troubles without blending),
+// evaluated by the update kernel on its tile + 1 halo from the troubles on
+// the tile + 3 halo, in eighths: w * 8 = 8, 6, 4, 3 and the ring 2 (all
+// exact, as is theta * 8 of the reference's float weights).
+//
+// A ghost cell's theta is the theta of its image (the reference fills the
+// ghosts of theta after computing it on the active cells). Outside a
+// periodic boundary that equals the theta evaluated in place, since the
+// troubles around it are periodic images too; outside a reflective or
+// zero-gradient boundary the image (one or two cells inside) lies in the
+// same tile and its value is used. The tile's own cells are written to
+// `theta_out` (the THETA field).
 // ---------------------------------------------------------------------------
-template <typename R, int D, int P, int TX, int TY, int TZ>
-__device__ __forceinline__ void fv_theta_kernel_body(const DevGrid& G, const uint8_t* __restrict__ T,
-                                                           uint8_t* __restrict__ theta, long long bidx) {
-    constexpr int n = P + 1;
-    using CB = CellBox<D, P, TX, TY, TZ>;
-    constexpr int E2x = TX * n + 4, E2y = TY * n + 4, E2z = D == 3 ? TZ * n + 4 : 1;
-    constexpr int E1x = TX * n + 2, E1y = TY * n + 2, E1z = D == 3 ? TZ * n + 2 : 1;
-    __shared__ uint8_t Ts[E2x * E2y * E2z];
-    __shared__ float Th[E1x * E1y * E1z];
-    int o[3];
-    {
-        int b = bidx;
-        const int tx = G.N[0] / TX, ty = G.N[1] / TY;
-        o[0] = (b % tx) * TX * n;
-        b /= tx;
-        o[1] = (b % ty) * TY * n;
-        b /= ty;
-        o[2] = D == 3 ? b * TZ * n : 0;
-    }
-    (void)CB::ext;
-    const int g2 = 2, gz2 = D == 3 ? 2 : 0;
-    for (int q = threadIdx.x; q < E2x * E2y * E2z; q += blockDim.x) {
-        int a[3] = {o[0] - g2 + q % E2x, o[1] - g2 + (q / E2x) % E2y, o[2] - gz2 + q / (E2x * E2y)};
-        bool fl[3];
-        Ts[q] = T[cell_image<D, P>(G, a, fl)];
-    }
-    __syncthreads();
-    if (!G.blending) {
-        for (int q = threadIdx.x; q < TX * n * TY * n * (D == 3 ? TZ * n : 1); q += blockDim.x) {
-            const int bx = TX * n, by = TY * n;
-            int a[3] = {q % bx, (q / bx) % by, q / (bx * by)};
-            const int s = (a[0] + 2) + E2x * ((a[1] + 2) + E2y * (a[2] + gz2));
-            int ga[3] = {o[0] + a[0], o[1] + a[1], o[2] + a[2]};
-            theta[cell_id<D, P>(G, ga)] = Ts[s] ? 8 : 0;
-        }
-        return;
-    }
-    const float w4[4] = {1.0f, 0.75f, 0.5f, 0.375f};
-    const int dz = D == 3 ? 1 : 0;
-    for (int q = threadIdx.x; q < E1x * E1y * E1z; q += blockDim.x) {
-        const int x = q % E1x + 1, y = (q / E1x) % E1y + 1, z = q / (E1x * E1y) + dz;
-        float th = 0;
-        for (int ok = -dz; ok <= dz; ok++)
-            for (int oj = -1; oj <= 1; oj++)
-                for (int oi = -1; oi <= 1; oi++) {
-                    const int n0 = (oi != 0) + (oj != 0) + (ok != 0);
-                    const float v = w4[n0] * (float)Ts[(x + oi) + E2x * ((y + oj) + E2y * (z + ok))];
-                    th = th < v ? v : th;
-                }
-        Th[q] = th;
-    }
-    __syncthreads();
-    const int bx = TX * n, by = TY * n, bz = D == 3 ? TZ * n : 1;
-    for (int q = threadIdx.x; q < bx * by * bz; q += blockDim.x) {
-        const int x = q % bx + 1, y = (q / bx) % by + 1, z = q / (bx * by) + dz;
-        const float th = Th[x + E1x * (y + E1y * z)];
-        float ring = 0;
-        for (int ok = -dz; ok <= dz; ok++)
-            for (int oj = -1; oj <= 1; oj++)
-                for (int oi = -1; oi <= 1; oi++)
-                    if (Th[(x + oi) + E1x * ((y + oj) + E1y * (z + ok))] > 0) ring = 0.25f;
-        const float t = th < ring ? ring : th;
-        int ga[3] = {o[0] + x - 1, o[1] + y - 1, o[2] + z - dz};
-        theta[cell_id<D, P>(G, ga)] = (uint8_t)(t * 8.0f);
-    }
-}
+template <int D, int P, int TX, int TY, int TZ>
+struct ThetaTile {
+    static constexpr int n = P + 1;
+    static constexpr int Bx = TX * n, By = TY * n, Bz = D == 3 ? TZ * n : 1;
+    static constexpr int E3x = Bx + 6, E3y = By + 6, E3z = D == 3 ? Bz + 6 : 1;
+    static constexpr int E2x = Bx + 4, E2y = By + 4, E2z = D == 3 ? Bz + 4 : 1;
+    static constexpr int E1x = Bx + 2, E1y = By + 2, E1z = D == 3 ? Bz + 2 : 1;
+    static constexpr int n3 = E3x * E3y * E3z, n2 = E2x * E2y * E2z, n1 = E1x * E1y * E1z;
+    static constexpr size_t scratch = (size_t)n3 + n2;  // bytes of T3 + Th2
+};
 
-template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_theta_kernel(DevGrid G, const uint8_t* __restrict__ T,
-                                                           uint8_t* __restrict__ theta) {
-    fv_theta_kernel_body<R, D, P, TX, TY, TZ>(G, T, theta, blockIdx.x);
+// called by every thread of the block; `scratch` holds ThetaTile::scratch
+// bytes; th (tile + 1 halo) is complete after the caller's next barrier
+template <int D, int P, int TX, int TY, int TZ>
+__device__ __forceinline__ void theta_on_tile(const DevGrid& G, const uint8_t* __restrict__ T, const int o[3],
+                                              uint8_t* scratch, uint8_t* th, uint8_t* __restrict__ theta_out) {
+    using TT = ThetaTile<D, P, TX, TY, TZ>;
+    constexpr int n = P + 1;
+    const int dz = D == 3 ? 1 : 0;
+    uint8_t* T3 = scratch;
+    uint8_t* Th2 = scratch + TT::n3;
+    for (int q = threadIdx.x; q < TT::n3; q += blockDim.x) {
+        int a[3] = {o[0] - 3 + q % TT::E3x, o[1] - 3 + (q / TT::E3x) % TT::E3y, o[2] - 3 * dz + q / (TT::E3x * TT::E3y)};
+        // a cell three layers outside a non-periodic boundary has no image
+        // (the ghost frame is two layers deep) and feeds no theta below:
+        // the theta of a ghost cell there is its image's
+        bool outside = false;
+#pragma unroll
+        for (int d = 0; d < D; d++)
+            outside |= G.bc[d] != kPeriodic && (a[d] < -2 || a[d] >= G.N[d] * n + 2);
+        bool fl[3];
+        T3[q] = outside ? (uint8_t)0 : T[cell_image<D, P>(G, a, fl)];
+    }
+    __syncthreads();
+    if (G.blending) {
+        for (int q = threadIdx.x; q < TT::n2; q += blockDim.x) {
+            const int x = q % TT::E2x + 1, y = (q / TT::E2x) % TT::E2y + 1, z = q / (TT::E2x * TT::E2y) + dz;
+            int m = 0;
+            for (int ok = -dz; ok <= dz; ok++)
+#pragma unroll
+                for (int oj = -1; oj <= 1; oj++)
+#pragma unroll
+                    for (int oi = -1; oi <= 1; oi++) {
+                        const int n0 = (oi != 0) + (oj != 0) + (ok != 0);
+                        const int w8 = n0 == 0 ? 8 : (n0 == 1 ? 6 : (n0 == 2 ? 4 : 3));
+                        if (T3[(x + oi) + TT::E3x * ((y + oj) + TT::E3y * (z + ok))]) m = m < w8 ? w8 : m;
+                    }
+            Th2[q] = (uint8_t)m;
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < TT::n1; q += blockDim.x) {
+        const int l0[3] = {q % TT::E1x, (q / TT::E1x) % TT::E1y, q / (TT::E1x * TT::E1y)};
+        int l[3] = {l0[0], l0[1], l0[2]};
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            const int a = o[d] - 1 + l[d], na = G.N[d] * n;
+            if ((a < 0 || a >= na) && G.bc[d] != kPeriodic) {
+                bool f = false;
+                l[d] = fv_image(a, na, G.bc[d], &f) - o[d] + 1;
+            }
+        }
+        int t8;
+        if (G.blending) {
+            const int x = l[0] + 1, y = l[1] + 1, z = l[2] + dz;
+            const int c = Th2[x + TT::E2x * (y + TT::E2y * z)];
+            int ring = 0;
+            for (int ok = -dz; ok <= dz; ok++)
+#pragma unroll
+                for (int oj = -1; oj <= 1; oj++)
+#pragma unroll
+                    for (int oi = -1; oi <= 1; oi++)
+                        if (Th2[(x + oi) + TT::E2x * ((y + oj) + TT::E2y * (z + ok))]) ring = 2;
+            t8 = c < ring ? ring : c;
+        } else {
+            t8 = T3[(l[0] + 2) + TT::E3x * ((l[1] + 2) + TT::E3y * (l[2] + 2 * dz))] ? 8 : 0;
+        }
+        th[q] = (uint8_t)t8;
+        const bool inner = l0[0] >= 1 && l0[0] <= TT::Bx && l0[1] >= 1 && l0[1] <= TT::By &&
+                           (D == 2 || (l0[2] >= 1 && l0[2] <= TT::Bz));
+        if (inner) {
+            int ga[3] = {o[0] + l0[0] - 1, o[1] + l0[1] - 1, o[2] + l0[2] - dz};
+            theta_out[cell_id<D, P>(G, ga)] = (uint8_t)t8;
+        }
+    }
 }
 
 // MUSCL-Hancock face states of cell X for a face of direction Dn
@@ -339,6 +497,12 @@ __device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], in
     }
 }
 
+// resident blocks the update kernel is compiled for: 5 (48 registers) in 2D,
+// where the extra warps hide its gather latency (measured on B200 at 256^2,
+// p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64)
+template <int D>
+constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : 1;
+
 template <typename R, int D, int P, int TX, int TY, int TZ>
 struct UpdateSmem {
     static constexpr int n = P + 1, V = D + 2;
@@ -355,6 +519,9 @@ struct UpdateSmem {
     static constexpr size_t wold = (size_t)E2x * E2y * E2z * V;
     static constexpr size_t epi = 2 * (size_t)NE * V * NPT;
     static constexpr size_t reals = faces + (wold > epi ? wold : epi);
+    static_assert(ThetaTile<D, P, TX, TY, TZ>::scratch <= (wold > epi ? wold : epi) * sizeof(R),
+                  "theta scratch fits the W_old area");
+    static_assert((size_t)NE * NPT * 16 + NE * 8 <= faces * sizeof(R), "indicator scratch fits the face area");
     static constexpr size_t bytes = reals * sizeof(R) + ((size_t)E1x * E1y * E1z + 15) / 16 * 16;
 };
 
@@ -400,12 +567,9 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
     const R dt = (R)(*A.dt);
     const R wdt = M.wt[A.t] * dt;
     const long long E = G.E;
-    // theta on the tile + 1 halo (ghost values are images)
-    for (int q = threadIdx.x; q < E1x * E1y * SM::E1z; q += blockDim.x) {
-        int a[3] = {o[0] - 1 + q % E1x, o[1] - 1 + (q / E1x) % E1y, o[2] - dz + q / (E1x * E1y)};
-        bool fl[3];
-        th[q] = A.theta[cell_image<D, P>(G, a, fl)];
-    }
+    // theta on the tile + 1 halo from the troubles (scratch: the W_old area,
+    // written only after the barrier that follows)
+    theta_on_tile<D, P, TX, TY, TZ>(G, A.trouble, o, reinterpret_cast<uint8_t*>(Wo), th, A.theta);
     // SD face fluxes of the tile
     const int nfaces[3] = {SM::NF0, SM::NF1, SM::NF2};
     int fbase[3] = {0, SM::NF0, SM::NF0 + SM::NF1};
@@ -579,6 +743,13 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
                 u[v] = val;
                 A.u[gi] = val;
             }
+            if (A.final_stage && A.feat) {
+                // (rho, p) of the new state for the indicator's features;
+                // the face-flux area is free now
+                double r, pr;
+                feature_rho_p(u, 1, V, G.gm, &r, &pr);
+                reinterpret_cast<double2*>(Fs)[q] = make_double2(r, pr);
+            }
             if (A.final_stage) {
                 R w[V];
                 primitives<D>(u, w, (R)G.gm);
@@ -588,6 +759,32 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
         }
         if (!A.final_stage) return;
         __syncthreads();
+        if (A.feat) {
+            // element means summed in point order, then the nodal features
+            // rho / mean - 1 and p / mean - 1 as BF16 (the values of the
+            // indicator's feature kernels)
+            const double2* RPs = reinterpret_cast<const double2*>(Fs);
+            float2* Mn = reinterpret_cast<float2*>(Fs) + 2 * SM::NE * NPT;
+            for (int el = threadIdx.x; el < SM::NE; el += blockDim.x) {
+                double sr = 0, sp = 0;
+                for (int pt = 0; pt < NPT; pt++) {
+                    sr = __dadd_rn(sr, RPs[el * NPT + pt].x);
+                    sp = __dadd_rn(sp, RPs[el * NPT + pt].y);
+                }
+                const float2 mn = make_float2((float)__ddiv_rn(sr, (double)NPT), (float)__ddiv_rn(sp, (double)NPT));
+                Mn[el] = mn;
+                A.means[el_ge[el]] = mn;
+            }
+            __syncthreads();
+            for (int q = threadIdx.x; q < SM::NE * NPT; q += blockDim.x) {
+                const int el = q / NPT, pt = q % NPT;
+                const double2 v = RPs[q];
+                const float2 mn = Mn[el];
+                uint16_t* row = A.feat + el_ge[el] * A.n_in;
+                row[pt] = bf16_bits(feature_ratio(v.x, mn.x));
+                row[NPT + pt] = bf16_bits(feature_ratio(v.y, mn.y));
+            }
+        }
         R* bufs2[2] = {(R*)src, Wsp};
         const R* s2 = Wsp;
         for (int d = 0; d < D; d++) {
@@ -613,7 +810,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D>) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
     fv_update_kernel_body<R, D, P, TX, TY, TZ>(G, M, A, blockIdx.x);
 }
 

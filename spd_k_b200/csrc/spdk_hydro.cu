@@ -147,9 +147,6 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
                 prof_begin(h);
                 k.detect<<<blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
                 prof_end(h, SPDK_KERNEL_DETECT);
-                prof_begin(h);
-                k.theta<<<blocks, kThreads, 0, h->stream>>>(h->G, h->trouble, h->theta);
-                prof_end(h, SPDK_KERNEL_THETA);
                 FallbackArgsT<R> F{};
                 F.ucv_in = ucv[t % 2];
                 F.ucv_out = ucv[(t + 1) % 2];
@@ -171,10 +168,15 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
                 F.wcv = (R*)h->wcv;
                 F.dtmin = h->dtmin;
                 F.dt = h->dt;
+                if (h->mlp && final_stage && t == h->nt - 1) {
+                    F.feat = h->feat;
+                    F.means = h->means;
+                    F.n_in = 2 * h->NPT + 4 * h->D;
+                }
                 prof_begin(h);
                 k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, dm, F);
                 prof_end(h, SPDK_KERNEL_UPDATE);
-                launches += 3;
+                launches += 2;
             }
         }
     }
@@ -187,23 +189,37 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
     return 0;
 }
 
+// the indicator's nodal features and element means of the current U, when
+// no step has left them (after creation, a write of U, or steps without the
+// indicator)
+int refresh_features(spdk_hydro* h) {
+    if (!h->mlp || h->feat_valid) return 0;
+    const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
+    const int rc = feature_rows(h->u, h->prec == SPDK_PRECISION_FP32, h->D, h->p, N, h->G.bc, h->G.gm, h->E,
+                                h->means, h->feat, h->stream);
+    if (!rc) h->feat_valid = true;
+    return rc;
+}
+
 int enqueue_step(spdk_hydro* h) {
     if (h->elem_trouble) SPDK_CUDA(cudaMemsetAsync(h->elem_trouble, 0, (size_t)h->E, h->stream));
     if (h->mlp) {
-        // a-priori indicator on the state at the start of the step, on the
-        // side stream (U is not written before the first detection)
+        if (int rc = refresh_features(h)) return rc;
+        // a-priori flags of the state at the start of the step, on the side
+        // stream, from the features the previous step's last update stored
+        // (they are not written again before the step's last update)
         SPDK_CUDA(cudaEventRecord(h->ev_fork, h->stream));
         SPDK_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
         const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
-        int rc = feature_rows(h->u, h->prec == SPDK_PRECISION_FP32, h->D, h->p, N, h->G.bc, h->G.gm, h->E, h->means,
-                              h->feat, h->side);
-        if (!rc) rc = mlp_infer_flags(h->mlp, h->feat, h->E, nullptr, h->elem_pred, h->thr, h->side);
+        const int rc = indicator_flags(h->mlp, h->feat, h->means, h->D, h->p, N, h->G.bc, h->E, h->elem_pred, h->thr,
+                                       h->side);
         if (rc) return rc;
         SPDK_CUDA(cudaEventRecord(h->ev_join, h->side));
         h->join_pending = true;
     }
     const int rc = h->prec == SPDK_PRECISION_FP32 ? enqueue_step_t<float>(h, h->ks32, h->dm32)
                                                   : enqueue_step_t<double>(h, h->ks64, h->dm64);
+    h->feat_valid = !rc && h->mlp != nullptr;
     return rc;
 }
 
@@ -449,8 +465,8 @@ int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info) {
     info->n_dof = h->E * h->NPT;
     info->n_time_slices = h->nt;
     int l = 0;
-    for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 3 * h->nt : 1);
-    info->launches_per_step = l + 1 + (h->mlp ? 3 : 0);
+    for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 2 * h->nt : 1);
+    info->launches_per_step = l + 1 + (h->mlp ? 2 : 0);
     info->device_bytes = h->bytes;
     return 0;
 }
@@ -478,6 +494,9 @@ int spdk_hydro_steps(spdk_hydro* h, int nsteps) {
     if (!h || nsteps < 0) return fail(SPDK_E_ARG, "bad argument");
     if (nsteps == 0) return 0;
     if (!h->graph) {
+        // features the captured step does not compute itself are formed
+        // before the capture, so every replay finds them current
+        if (int rc = refresh_features(h)) return rc;
         // capture one step; replays reuse the same device pointers
         cudaGraph_t g;
         SPDK_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -489,6 +508,7 @@ int spdk_hydro_steps(spdk_hydro* h, int nsteps) {
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
     }
+    if (int rc = refresh_features(h)) return rc;
     for (int s = 0; s < nsteps; s++) SPDK_CUDA(cudaGraphLaunch(h->graph, h->stream));
     return 0;
 }
@@ -607,6 +627,7 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     if (field != SPDK_FIELD_U_SP) return fail(SPDK_E_ARG, "only U_sp can be written");
     if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
     const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+    h->feat_valid = false;
     if (h->prec == SPDK_PRECISION_FP32) {
         // doubles rounded once to FP32
         std::vector<float> b(host, host + state);
@@ -672,6 +693,7 @@ int spdk_hydro_set_indicator(spdk_hydro* h, spdk_mlp* m, float threshold) {
     }
     h->mlp = m;
     h->thr = threshold;
+    h->feat_valid = false;
     h->G.elem_pred = m ? h->elem_pred : nullptr;
     // the captured step holds the old kernel arguments
     if (h->graph) {

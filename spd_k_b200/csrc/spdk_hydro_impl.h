@@ -50,6 +50,9 @@ struct spdk_hydro {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool join_pending = false;
+    // feat / means hold the nodal features and element means of the current
+    // U (the last update of a step with the indicator writes them)
+    bool feat_valid = false;
     size_t bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;

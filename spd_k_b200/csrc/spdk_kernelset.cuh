@@ -97,7 +97,6 @@ struct KernelSetT {
     void (*correct)(DevGrid, DevMatsT<R>, PicardArgsT<R>) = nullptr;
     void (*flux)(DevGrid, DevMatsT<R>, PicardArgsT<R>) = nullptr;
     void (*detect)(DevGrid, const double2*, const double2*, uint8_t*, int*) = nullptr;
-    void (*theta)(DevGrid, const uint8_t*, uint8_t*) = nullptr;
     void (*update)(DevGrid, DevMatsT<R>, FallbackArgsT<R>) = nullptr;
     void (*init)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
     void (*derive)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
@@ -113,7 +112,6 @@ KernelSetT<R> make_set() {
     k.correct = picard_kernel<R, D, P, TX, TY, TZ, kCorrect>;
     k.flux = picard_kernel<R, D, P, TX, TY, TZ, kFlux>;
     k.detect = fv_detect_kernel<R, D, P, TX, TY, TZ>;
-    k.theta = fv_theta_kernel<R, D, P, TX, TY, TZ>;
     k.update = fv_update_kernel<R, D, P, TX, TY, TZ>;
     k.init = init_state_kernel<R, D, P>;
     k.derive = derive_kernel<R, D, P>;

@@ -19,6 +19,7 @@
 #include "spdk.h"
 #include "spdk_learned.h"
 #include "spdk_learned_impl.h"
+#include "spdk_physics.cuh"
 
 namespace spdk {
 int fail(int code, const std::string& msg);
@@ -170,110 +171,6 @@ __global__ void __launch_bounds__(kThreadsM) k_mlp_forward(int n_in, const uint1
     }
 }
 
-// Inference: a persistent grid; each block keeps the parameters in shared
-// memory and walks tiles of 128 samples, each thread accumulating 4 hidden
-// units x 8 samples in registers (12 shared loads per 32 FMAs). The sums
-// run over k in the same order as forward_tile, so the probabilities are
-// the same as the training kernels'.
-constexpr int kSI = 128;  // samples per inference tile
-constexpr size_t kInferSmemMax = 200 * 1024;
-struct InferSmem {
-    int wbytes, xoff, h1, total;
-};
-__host__ __device__ inline InferSmem infer_smem(int n_in) {
-    const Layout L = layout(n_in);
-    InferSmem s;
-    s.wbytes = ((L.n * 2 + 15) / 16) * 16;
-    s.xoff = s.wbytes;
-    s.h1 = s.xoff + kSI * n_in * 4;
-    s.total = s.h1 + kSI * kH * 4;
-    return s;
-}
-
-__global__ void __launch_bounds__(kThreadsM) k_mlp_infer(int n_in, const uint16_t* __restrict__ wbf,
-                                                           const uint16_t* __restrict__ x, long long batch,
-                                                           float* __restrict__ p, uint8_t* __restrict__ flags,
-                                                           float thr) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    const Layout L = layout(n_in);
-    const InferSmem S = infer_smem(n_in);
-    load_params(L, sm, wbf);
-    const uint16_t* W = reinterpret_cast<const uint16_t*>(sm);
-    float* X = reinterpret_cast<float*>(sm + S.xoff);
-    float* H1 = reinterpret_cast<float*>(sm + S.h1);
-    const int j0 = threadIdx.x % 16, g = threadIdx.x / 16;  // units j0 + 16u, samples g + 16r
-    const long long tiles = (batch + kSI - 1) / kSI;
-    for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const long long s0 = tile * kSI;
-        for (int q = threadIdx.x; q < kSI * n_in; q += blockDim.x) {
-            const int s = q / n_in, k = q % n_in;
-            X[q] = (s0 + s < batch) ? bf(x[(s0 + s) * n_in + k]) : 0.0f;
-        }
-        __syncthreads();
-        // two hidden layers: in [kSI][nk] -> gelu(in W + b); the first goes
-        // to H1, the second straight into the output dot product
-        float zp[8];
-        for (int layer = 0; layer < 2; layer++) {
-            const float* in = layer == 0 ? X : H1;
-            const int nk = layer == 0 ? n_in : kH;
-            const int oW = layer == 0 ? L.oW1 : L.oW2, ob = layer == 0 ? L.ob1 : L.ob2;
-            float acc[8][4];
-#pragma unroll
-            for (int r = 0; r < 8; r++)
-#pragma unroll
-                for (int u = 0; u < 4; u++) acc[r][u] = 0.0f;
-            for (int k = 0; k < nk; k++) {
-                float w[4], xv[8];
-#pragma unroll
-                for (int u = 0; u < 4; u++) w[u] = bf(W[oW + k * kH + j0 + 16 * u]);
-#pragma unroll
-                for (int r = 0; r < 8; r++) xv[r] = in[(g + 16 * r) * nk + k];
-#pragma unroll
-                for (int r = 0; r < 8; r++)
-#pragma unroll
-                    for (int u = 0; u < 4; u++) acc[r][u] += xv[r] * w[u];
-            }
-            if (layer == 0) {
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const float b = bf(W[ob + j0 + 16 * u]);
-#pragma unroll
-                    for (int r = 0; r < 8; r++) H1[(g + 16 * r) * kH + j0 + 16 * u] = gelu(acc[r][u] + b);
-                }
-                __syncthreads();
-            } else {
-                // this thread's 4 units of w3 . H2 for its 8 samples, then the
-                // 16 threads of a sample group (consecutive lanes) add up
-#pragma unroll
-                for (int r = 0; r < 8; r++) zp[r] = 0.0f;
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const float b = bf(W[ob + j0 + 16 * u]), w3 = bf(W[L.ow3 + j0 + 16 * u]);
-#pragma unroll
-                    for (int r = 0; r < 8; r++) zp[r] += gelu(acc[r][u] + b) * w3;
-                }
-#pragma unroll
-                for (int r = 0; r < 8; r++)
-#pragma unroll
-                    for (int off = 8; off > 0; off >>= 1) zp[r] += __shfl_xor_sync(0xffffffffu, zp[r], off);
-            }
-        }
-        if (j0 == 0) {
-            const float b3 = bf(W[L.ob3]);
-#pragma unroll
-            for (int r = 0; r < 8; r++) {
-                const long long s = s0 + g + 16 * r;
-                if (s < batch) {
-                    const float pr = 1.0f / (1.0f + expf(-(zp[r] + b3)));
-                    if (p) p[s] = pr;
-                    if (flags) flags[s] = pr > thr ? 1 : 0;
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
 // per block: sum_s w_s BCE_s, sum_s w_s and the unnormalised gradient
 // sum_s w_s dBCE_s/dtheta into part[block][0 .. n+1]
 __global__ void __launch_bounds__(kThreadsM) k_mlp_grad(int n_in, const uint16_t* __restrict__ wbf,
@@ -415,14 +312,7 @@ __global__ void k_to_bf16(const float* __restrict__ w, uint16_t* __restrict__ wb
 // ---- feature rows of a solver state -----------------------------------------
 template <typename R>
 __device__ __forceinline__ void rho_p_point(const R* u, int V, int NPT, int pt, double gm, double* rho, double* p) {
-    const double r = (double)u[pt];
-    double m2 = 0;
-    for (int d = 1; d < V - 1; d++) {
-        const double m = (double)u[d * NPT + pt];
-        m2 += m * m;
-    }
-    *rho = r;
-    *p = ((double)u[(V - 1) * NPT + pt] - 0.5 * m2 / r) * (gm - 1.0);
+    feature_rho_p(u + pt, NPT, V, gm, rho, p);
 }
 
 // per element: mean density and mean pressure over the solution points,
@@ -451,53 +341,353 @@ __global__ void k_elem_means(const R* __restrict__ u, int V, int NPT, long long 
     }
 }
 
-__device__ __forceinline__ float safe_ratio(double a, double b) {
-    const double r = (b > 0 && isfinite(b)) ? a / b - 1.0 : 0.0;
-    return isfinite(r) ? (float)r : 0.0f;
+__device__ __forceinline__ float safe_ratio(double a, double b) { return feature_ratio(a, b); }
+
+// element grid of a feature row
+struct FeatureGeom {
+    int D, V, NPT;
+    int N[3], bc[3];
+    long long E;
+};
+
+// the nodal part of element e's row at point pt: rho / mean - 1 (column
+// pt) and p / mean - 1 (column NPT + pt)
+template <typename R>
+__device__ __forceinline__ void own_features(const R* __restrict__ u, const float2* __restrict__ mean,
+                                             const FeatureGeom& F, double gm, long long e, int pt, uint16_t* xr,
+                                             uint16_t* xp) {
+    double r, p;
+    rho_p_point(u + e * F.V * F.NPT, F.V, F.NPT, pt, gm, &r, &p);
+    const float2 me = mean[e];
+    *xr = to_bf(safe_ratio(r, me.x));
+    *xp = to_bf(safe_ratio(p, me.y));
+}
+
+// min and max over the two neighbours of a direction of the ratio of their
+// mean to the element's, for rho then p
+__device__ __forceinline__ void neighbour_values(float2 me, float2 lo, float2 hi, uint16_t f[4]) {
+    const float r0 = safe_ratio(lo.x, me.x), r1 = safe_ratio(hi.x, me.x);
+    const float p0 = safe_ratio(lo.y, me.y), p1 = safe_ratio(hi.y, me.y);
+    f[0] = to_bf(fminf(r0, r1));
+    f[1] = to_bf(fmaxf(r0, r1));
+    f[2] = to_bf(fminf(p0, p1));
+    f[3] = to_bf(fmaxf(p0, p1));
+}
+
+// the neighbour part of direction d (columns 2 NPT + 4d ..): min and max
+// over the two neighbours of the ratio of their mean to the element's, for
+// rho then p; outside a non-periodic boundary the neighbour is the element
+__device__ __forceinline__ void neighbour_features(const float2* __restrict__ mean, const FeatureGeom& F,
+                                                   long long e, int d, uint16_t f[4]) {
+    const float2 me = mean[e];
+    const int c[3] = {(int)(e % F.N[0]), (int)((e / F.N[0]) % F.N[1]), (int)(e / ((long long)F.N[0] * F.N[1]))};
+    float2 nb[2];
+    for (int sd = 0; sd < 2; sd++) {
+        int cc[3] = {c[0], c[1], c[2]};
+        cc[d] += sd ? 1 : -1;
+        if (cc[d] < 0 || cc[d] >= F.N[d]) {
+            if (F.bc[d] == SPDK_BC_PERIODIC) cc[d] = cc[d] < 0 ? cc[d] + F.N[d] : cc[d] - F.N[d];
+            else cc[d] = c[d];
+        }
+        nb[sd] = mean[((long long)cc[2] * F.N[1] + cc[1]) * F.N[0] + cc[0]];
+    }
+    neighbour_values(me, nb[0], nb[1], f);
 }
 
 // feature rows: the nodal part one thread per (element, point), the
 // neighbour part one thread per (element, direction)
 template <typename R>
-__global__ void k_features(const R* __restrict__ u, const float2* __restrict__ mean, int D, int V, int NPT, int N0,
-                           int N1, int N2, int bc0, int bc1, int bc2, long long E, double gm, int n_in,
-                           uint16_t* __restrict__ x) {
+__global__ void k_features(const R* __restrict__ u, const float2* __restrict__ mean, FeatureGeom F, double gm,
+                           int n_in, uint16_t* __restrict__ x) {
+    const int NPT = F.NPT, D = F.D;
     const int per = NPT >= (int)blockDim.x ? 1 : (int)blockDim.x / NPT;
     const long long e0 = (long long)blockIdx.x * per;
     for (int q = threadIdx.x; q < per * NPT; q += blockDim.x) {
         const int el = q / NPT, pt = q % NPT;
         const long long e = e0 + el;
-        if (e >= E) continue;
-        double r, p;
-        rho_p_point(u + e * V * NPT, V, NPT, pt, gm, &r, &p);
-        const float2 me = mean[e];
-        x[e * n_in + pt] = to_bf(safe_ratio(r, me.x));
-        x[e * n_in + NPT + pt] = to_bf(safe_ratio(p, me.y));
+        if (e >= F.E) continue;
+        own_features(u, mean, F, gm, e, pt, &x[e * n_in + pt], &x[e * n_in + NPT + pt]);
     }
     for (int q = threadIdx.x; q < per * D; q += blockDim.x) {
         const long long e = e0 + q / D;
         const int d = q % D;
-        if (e >= E) continue;
-        const float2 me = mean[e];
-        const int N[3] = {N0, N1, N2}, bc[3] = {bc0, bc1, bc2};
-        const int c[3] = {(int)(e % N0), (int)((e / N0) % N1), (int)(e / ((long long)N0 * N1))};
-        float2 nb[2];
-        for (int sd = 0; sd < 2; sd++) {
-            int cc[3] = {c[0], c[1], c[2]};
-            cc[d] += sd ? 1 : -1;
-            if (cc[d] < 0 || cc[d] >= N[d]) {
-                if (bc[d] == SPDK_BC_PERIODIC) cc[d] = cc[d] < 0 ? cc[d] + N[d] : cc[d] - N[d];
-                else cc[d] = c[d];  // outside the domain: the element itself
-            }
-            nb[sd] = mean[((long long)cc[2] * N1 + cc[1]) * N0 + cc[0]];
+        if (e >= F.E) continue;
+        neighbour_features(mean, F, e, d, x + e * n_in + 2 * NPT + 4 * d);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Inference on the tensor cores: mma.sync m16n8k16 with BF16 operands and
+// FP32 accumulators, one warp per 16 samples.
+//
+// Layer 1 takes the BF16 input rows (staged in shared memory) as the A
+// operand and W1 as B. Its FP32 accumulators, after bias and GELU, are held
+// in the layout of an m16n8k16 A operand (n-tiles 2c and 2c+1 of layer 1 are
+// k-chunk c of layer 2), and each activation is split exactly into three
+// BF16 terms (hi + mid + lo == the FP32 value; each residual has at most 16
+// and then 8 significant bits), so layer 2 multiplies the same FP32
+// activations as the training kernels, with products exact in FP32. The
+// output layer is a dot product over the accumulators reduced across the 4
+// lanes of a quad. Only the accumulation order differs from forward_tile.
+//
+// B fragments are pre-arranged in shared memory in lane order (one 8-byte
+// load per lane per fragment, no bank conflicts); input rows have a stride
+// of 16 kc + 8 BF16 (an odd multiple of 4 words), which makes the A-fragment
+// loads conflict-free too.
+// ---------------------------------------------------------------------------
+constexpr int kTcWarps = 8;
+
+struct TcSmem {
+    int kc1, ldx, w1f, w2f, vec, xs, total;
+};
+__host__ __device__ inline TcSmem tc_smem(int n_in, int warps) {
+    TcSmem s;
+    s.kc1 = (n_in + 15) / 16;
+    s.ldx = s.kc1 * 16 + 8;
+    s.w1f = 0;                              // uint2 [kc1][8 n-tiles][32 lanes]
+    s.w2f = s.w1f + s.kc1 * 8 * 32 * 8;     // uint2 [4][8][32]
+    s.vec = s.w2f + 4 * 8 * 32 * 8;         // float b1[kH], b2[kH], w3[kH], b3 (+3 pad)
+    s.xs = s.vec + (3 * kH + 4) * 4;        // uint16 [warps][16][ldx]
+    s.total = s.xs + warps * 16 * s.ldx * 2;
+    return s;
+}
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t pack_bf(uint16_t lo, uint16_t hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
+
+// x == bf(h) + bf(m) + bf(l) exactly (round-to-nearest residuals)
+__device__ __forceinline__ void split3(float x, uint16_t* h, uint16_t* m, uint16_t* l) {
+    *h = to_bf(x);
+    const float r1 = x - bf(*h);
+    *m = to_bf(r1);
+    *l = to_bf(r1 - bf(*m));
+}
+
+// B fragments of W1 (k < n_in, zero beyond) and W2, and the FP32 vectors
+__device__ void load_tc_params(const Layout& L, const TcSmem& S, unsigned char* sm, const uint16_t* __restrict__ wbf) {
+    uint2* W1f = reinterpret_cast<uint2*>(sm + S.w1f);
+    uint2* W2f = reinterpret_cast<uint2*>(sm + S.w2f);
+    float* vec = reinterpret_cast<float*>(sm + S.vec);
+    const int n1 = S.kc1 * 8 * 32, n2 = 4 * 8 * 32;
+    for (int q = threadIdx.x; q < n1 + n2; q += blockDim.x) {
+        const bool first = q < n1;
+        const int r = first ? q : q - n1;
+        const int lane = r % 32, nt = (r / 32) % 8, kc = r / 256;
+        const int g = lane >> 2, t = lane & 3;
+        const int nk = first ? L.n_in : kH, oW = first ? L.oW1 : L.oW2;
+        const int col = nt * 8 + g;
+        const int k0 = kc * 16 + 2 * t;
+        uint16_t v[4];
+        const int ks[4] = {k0, k0 + 1, k0 + 8, k0 + 9};
+#pragma unroll
+        for (int i = 0; i < 4; i++) v[i] = ks[i] < nk ? wbf[oW + ks[i] * kH + col] : (uint16_t)0;
+        (first ? W1f : W2f)[r] = make_uint2(pack_bf(v[0], v[1]), pack_bf(v[2], v[3]));
+    }
+    for (int q = threadIdx.x; q < kH; q += blockDim.x) {
+        vec[q] = bf(wbf[L.ob1 + q]);
+        vec[kH + q] = bf(wbf[L.ob2 + q]);
+        vec[2 * kH + q] = bf(wbf[L.ow3 + q]);
+    }
+    if (threadIdx.x == 0) vec[3 * kH] = bf(wbf[L.ob3]);
+    __syncthreads();
+}
+
+// the network on the warp's 16 rows in Xs ([16][ldx] BF16); z[0], z[1] are
+// the logits of rows g and g + 8 (g = lane / 4), in every lane of the quad
+__device__ __forceinline__ void mlp16_tc(const TcSmem& S, const unsigned char* sm, const uint16_t* Xs, float z[2]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const uint2* W1f = reinterpret_cast<const uint2*>(sm + S.w1f);
+    const uint2* W2f = reinterpret_cast<const uint2*>(sm + S.w2f);
+    const float* vec = reinterpret_cast<const float*>(sm + S.vec);
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc[nt][i] = 0.0f;
+    for (int kc = 0; kc < S.kc1; kc++) {
+        const uint16_t* x0 = Xs + g * S.ldx + kc * 16 + 2 * t;
+        const uint32_t a[4] = {*reinterpret_cast<const uint32_t*>(x0),
+                               *reinterpret_cast<const uint32_t*>(x0 + 8 * S.ldx),
+                               *reinterpret_cast<const uint32_t*>(x0 + 8),
+                               *reinterpret_cast<const uint32_t*>(x0 + 8 * S.ldx + 8)};
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const uint2 b = W1f[(kc * 8 + nt) * 32 + lane];
+            mma_bf16(acc[nt], a, b.x, b.y);
         }
-        const float r0 = safe_ratio(nb[0].x, me.x), r1 = safe_ratio(nb[1].x, me.x);
-        const float p0 = safe_ratio(nb[0].y, me.y), p1 = safe_ratio(nb[1].y, me.y);
-        uint16_t* row = x + e * n_in + 2 * NPT + 4 * d;
-        row[0] = to_bf(fminf(r0, r1));
-        row[1] = to_bf(fmaxf(r0, r1));
-        row[2] = to_bf(fminf(p0, p1));
-        row[3] = to_bf(fmaxf(p0, p1));
+    }
+    // H1 = gelu(A1 + b1), in place: acc[nt][0..1] row g, [2..3] row g + 8,
+    // columns nt * 8 + 2t + {0, 1}
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int c0 = nt * 8 + 2 * t;
+        acc[nt][0] = gelu(acc[nt][0] + vec[c0]);
+        acc[nt][1] = gelu(acc[nt][1] + vec[c0 + 1]);
+        acc[nt][2] = gelu(acc[nt][2] + vec[c0]);
+        acc[nt][3] = gelu(acc[nt][3] + vec[c0 + 1]);
+    }
+    float acc2[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) acc2[nt][i] = 0.0f;
+#pragma unroll
+    for (int kc = 0; kc < 4; kc++) {
+        // A registers of k-chunk kc: {row g, cols 2t..}, {row g+8}, {row g, cols 8+2t..}, {row g+8, 8+}
+        uint32_t ah[4], am[4], al[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const float* hp = acc[2 * kc + (r >> 1)] + 2 * (r & 1);
+            uint16_t h0, m0, l0, h1, m1, l1;
+            split3(hp[0], &h0, &m0, &l0);
+            split3(hp[1], &h1, &m1, &l1);
+            ah[r] = pack_bf(h0, h1);
+            am[r] = pack_bf(m0, m1);
+            al[r] = pack_bf(l0, l1);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const uint2 b = W2f[(kc * 8 + nt) * 32 + lane];
+            mma_bf16(acc2[nt], al, b.x, b.y);
+            mma_bf16(acc2[nt], am, b.x, b.y);
+            mma_bf16(acc2[nt], ah, b.x, b.y);
+        }
+    }
+    float z0 = 0.0f, z1 = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int c0 = nt * 8 + 2 * t;
+        z0 += gelu(acc2[nt][0] + vec[kH + c0]) * vec[2 * kH + c0];
+        z0 += gelu(acc2[nt][1] + vec[kH + c0 + 1]) * vec[2 * kH + c0 + 1];
+        z1 += gelu(acc2[nt][2] + vec[kH + c0]) * vec[2 * kH + c0];
+        z1 += gelu(acc2[nt][3] + vec[kH + c0 + 1]) * vec[2 * kH + c0 + 1];
+    }
+    z0 += __shfl_xor_sync(0xffffffffu, z0, 1);
+    z0 += __shfl_xor_sync(0xffffffffu, z0, 2);
+    z1 += __shfl_xor_sync(0xffffffffu, z1, 1);
+    z1 += __shfl_xor_sync(0xffffffffu, z1, 2);
+    z[0] = z0 + vec[3 * kH];
+    z[1] = z1 + vec[3 * kH];
+}
+
+// true when the warp's 16 staged rows are all zero (columns < n_in)
+__device__ __forceinline__ bool tile_is_zero(const TcSmem& S, const uint16_t* Xs, int n_in) {
+    const int lane = threadIdx.x & 31;
+    bool nz = false;
+    for (int q = lane; q < 16 * n_in; q += 32) {
+        const int row = q / n_in, k = q - row * n_in;
+        nz |= Xs[row * S.ldx + k] != 0;
+    }
+    return !__any_sync(0xffffffffu, nz);
+}
+
+__device__ __forceinline__ void write_outputs(const float z[2], long long s0, long long batch, float* __restrict__ p,
+                                              uint8_t* __restrict__ flags, float thr) {
+    const int lane = threadIdx.x & 31;
+    if ((lane & 3) != 0) return;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const long long s = s0 + (lane >> 2) + 8 * h;
+        if (s < batch) {
+            const float pr = 1.0f / (1.0f + expf(-z[h]));
+            if (p) p[s] = pr;
+            if (flags) flags[s] = pr > thr ? 1 : 0;
+        }
+    }
+}
+
+// probabilities / flags of BF16 feature rows x [batch][n_in]
+__global__ void __launch_bounds__(kTcWarps * 32) k_mlp_infer_tc(int n_in, const uint16_t* __restrict__ wbf,
+                                                                const float* __restrict__ z0,
+                                                                const uint16_t* __restrict__ x, long long batch,
+                                                                float* __restrict__ p, uint8_t* __restrict__ flags,
+                                                                float thr) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const Layout L = layout(n_in);
+    const TcSmem S = tc_smem(n_in, kTcWarps);
+    load_tc_params(L, S, sm, wbf);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint16_t* Xs = reinterpret_cast<uint16_t*>(sm + S.xs) + warp * 16 * S.ldx;
+    for (int q = lane; q < 16 * S.ldx; q += 32) Xs[q] = 0;  // padding columns stay zero
+    __syncwarp();
+    const float zz = *z0;
+    const long long tiles = (batch + 15) / 16;
+    for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles; tile += (long long)gridDim.x * kTcWarps) {
+        const long long s0 = tile * 16;
+        for (int q = lane; q < 16 * n_in; q += 32) {
+            const int row = q / n_in, k = q - row * n_in;
+            Xs[row * S.ldx + k] = s0 + row < batch ? x[(s0 + row) * n_in + k] : (uint16_t)0;
+        }
+        __syncwarp();
+        float z[2] = {zz, zz};
+        if (!tile_is_zero(S, Xs, n_in)) mlp16_tc(S, sm, Xs, z);
+        write_outputs(z, s0, batch, p, flags, thr);
+        __syncwarp();  // the next tile overwrites Xs
+    }
+}
+
+// the logit of the all-zero input row, *z0 (one warp): a tile whose rows
+// are all zero gives it for every row, so the inference kernels reuse it;
+// recomputed whenever the BF16 weights change
+__global__ void __launch_bounds__(32) k_mlp_zero_logit(int n_in, const uint16_t* __restrict__ wbf, float* z0) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const Layout L = layout(n_in);
+    const TcSmem S = tc_smem(n_in, 1);
+    load_tc_params(L, S, sm, wbf);
+    uint16_t* Xs = reinterpret_cast<uint16_t*>(sm + S.xs);
+    for (int q = threadIdx.x; q < 16 * S.ldx; q += 32) Xs[q] = 0;
+    __syncwarp();
+    float z[2];
+    mlp16_tc(S, sm, Xs, z);
+    if (threadIdx.x == 0) *z0 = z[0];
+}
+
+// the solver's a-priori flags from its stored feature rows: the nodal part
+// of each row (columns < 2 NPT, written by the step's last update) and the
+// neighbour part formed here from the element means; one warp per 16
+// elements
+__global__ void __launch_bounds__(kTcWarps * 32) k_indicator_rows_tc(const uint16_t* __restrict__ feat,
+                                                                     const float2* __restrict__ mean, FeatureGeom F,
+                                                                     int n_in, const uint16_t* __restrict__ wbf,
+                                                                     const float* __restrict__ z0,
+                                                                     uint8_t* __restrict__ flags, float thr) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const Layout L = layout(n_in);
+    const TcSmem S = tc_smem(n_in, kTcWarps);
+    load_tc_params(L, S, sm, wbf);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint16_t* Xs = reinterpret_cast<uint16_t*>(sm + S.xs) + warp * 16 * S.ldx;
+    for (int q = lane; q < 16 * S.ldx; q += 32) Xs[q] = 0;
+    __syncwarp();
+    const float zz = *z0;
+    const int nod = 2 * F.NPT;
+    const long long tiles = (F.E + 15) / 16;
+    for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles; tile += (long long)gridDim.x * kTcWarps) {
+        const long long e0 = tile * 16;
+        for (int q = lane; q < 16 * nod; q += 32) {
+            const int row = q / nod, k = q - row * nod;
+            Xs[row * S.ldx + k] = e0 + row < F.E ? feat[(e0 + row) * n_in + k] : (uint16_t)0;
+        }
+        for (int q = lane; q < 16 * F.D; q += 32) {
+            const int row = q / F.D, d = q - row * F.D;
+            const long long e = e0 + row;
+            uint16_t f[4] = {0, 0, 0, 0};
+            if (e < F.E) neighbour_features(mean, F, e, d, f);
+#pragma unroll
+            for (int i = 0; i < 4; i++) Xs[row * S.ldx + nod + 4 * d + i] = f[i];
+        }
+        __syncwarp();
+        float z[2] = {zz, zz};
+        if (!tile_is_zero(S, Xs, n_in)) mlp16_tc(S, sm, Xs, z);
+        write_outputs(z, e0, F.E, nullptr, flags, thr);
+        __syncwarp();
     }
 }
 
@@ -515,44 +705,79 @@ struct spdk_mlp {
     uint16_t* wbf = nullptr;
     int part_blocks = 0;
     long long step = 0;
-    size_t smem = 0, infer_smem = 0;
+    size_t smem = 0, tc_smem = 0, z0_smem = 0;
+    float* z0 = nullptr;  // logit of the all-zero input row (device)
 };
 
 namespace spdk {
 
+static FeatureGeom geom(int D, int p, const int N[3], const int bc[3], long long E) {
+    FeatureGeom F;
+    const int n = p + 1;
+    F.D = D;
+    F.V = D + 2;
+    F.NPT = D == 2 ? n * n : n * n * n;
+    for (int d = 0; d < 3; d++) {
+        F.N[d] = N[d];
+        F.bc[d] = bc[d];
+    }
+    F.E = E;
+    return F;
+}
+
+static int launch_means(const void* u, bool fp32, const FeatureGeom& F, double gm, float2* means, cudaStream_t s) {
+    const int threads = 256;
+    const int per = F.NPT >= threads ? 1 : threads / F.NPT;
+    const unsigned g = (unsigned)((F.E + per - 1) / per);
+    const size_t sm = (size_t)per * F.NPT * sizeof(double2);
+    if (fp32) k_elem_means<float><<<g, threads, sm, s>>>((const float*)u, F.V, F.NPT, F.E, gm, means);
+    else k_elem_means<double><<<g, threads, sm, s>>>((const double*)u, F.V, F.NPT, F.E, gm, means);
+    return 0;
+}
+
+static unsigned tc_blocks(long long rows) {
+    const long long tiles = (rows + 15) / 16;
+    const long long b = (tiles + kTcWarps - 1) / kTcWarps;
+    return (unsigned)(b < 148LL * 4 ? (b < 1 ? 1 : b) : 148LL * 4);
+}
+
 int mlp_infer_flags(spdk_mlp* m, const uint16_t* x, long long batch, float* p, uint8_t* flags, float thr,
                     cudaStream_t s) {
-    if (m->infer_smem <= kInferSmemMax) {
-        const long long tiles = (batch + kSI - 1) / kSI;
-        const unsigned blocks = (unsigned)(tiles < 148LL * 2 ? tiles : 148LL * 2);
-        k_mlp_infer<<<blocks, kThreadsM, m->infer_smem, s>>>(m->n_in, m->wbf, x, batch, p, flags, thr);
-    } else {
-        // wide inputs (3D, high order): the 32-sample tiles of the training kernels
-        const unsigned blocks = (unsigned)((batch + kSB - 1) / kSB);
-        k_mlp_forward<<<blocks, kThreadsM, m->smem, s>>>(m->n_in, m->wbf, x, (int)batch, p, flags, thr);
-    }
+    k_mlp_infer_tc<<<tc_blocks(batch), kTcWarps * 32, m->tc_smem, s>>>(m->n_in, m->wbf, m->z0, x, batch, p, flags,
+                                                                       thr);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("indicator: ") + cudaGetErrorString(e));
 }
 
 int feature_rows(const void* u, bool fp32, int D, int p, const int N[3], const int bc[3], double gm, long long E,
                  float2* means, uint16_t* x, cudaStream_t s) {
-    const int n = p + 1, NPT = D == 2 ? n * n : n * n * n, V = D + 2, n_in = 2 * NPT + 4 * D;
+    const FeatureGeom F = geom(D, p, N, bc, E);
+    const int n_in = 2 * F.NPT + 4 * D;
+    launch_means(u, fp32, F, gm, means, s);
     const int threads = 256;
-    const int per = NPT >= threads ? 1 : threads / NPT;
+    const int per = F.NPT >= threads ? 1 : threads / F.NPT;
     const unsigned g = (unsigned)((E + per - 1) / per);
-    const size_t sm = (size_t)per * NPT * sizeof(double2);
-    if (fp32) {
-        k_elem_means<float><<<g, threads, sm, s>>>((const float*)u, V, NPT, E, gm, means);
-        k_features<float><<<g, threads, 0, s>>>((const float*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1],
-                                                 bc[2], E, gm, n_in, x);
-    } else {
-        k_elem_means<double><<<g, threads, sm, s>>>((const double*)u, V, NPT, E, gm, means);
-        k_features<double><<<g, threads, 0, s>>>((const double*)u, means, D, V, NPT, N[0], N[1], N[2], bc[0], bc[1],
-                                                  bc[2], E, gm, n_in, x);
-    }
+    if (fp32) k_features<float><<<g, threads, 0, s>>>((const float*)u, means, F, gm, n_in, x);
+    else k_features<double><<<g, threads, 0, s>>>((const double*)u, means, F, gm, n_in, x);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("features: ") + cudaGetErrorString(e));
+}
+
+int indicator_flags(spdk_mlp* m, const uint16_t* feat, const float2* means, int D, int p, const int N[3],
+                    const int bc[3], long long E, uint8_t* flags, float thr, cudaStream_t s) {
+    const FeatureGeom F = geom(D, p, N, bc, E);
+    if (2 * F.NPT + 4 * D != m->n_in) return fail(SPDK_E_ARG, "indicator input width does not match the solver");
+    k_indicator_rows_tc<<<tc_blocks(E), kTcWarps * 32, m->tc_smem, s>>>(feat, means, F, m->n_in, m->wbf, m->z0, flags,
+                                                                        thr);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("indicator: ") + cudaGetErrorString(e));
+}
+
+// the zero-input logit after a change of the BF16 weights
+static int update_zero_logit(spdk_mlp* m, cudaStream_t s) {
+    k_mlp_zero_logit<<<1, 32, m->z0_smem, s>>>(m->n_in, m->wbf, m->z0);
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("mlp zero logit: ") + cudaGetErrorString(e));
 }
 
 int mlp_n_in(const spdk_mlp* m) { return m->n_in; }
@@ -571,7 +796,8 @@ int spdk_mlp_create(int n_in, int hidden, unsigned long long seed, spdk_mlp** ou
     const Layout L = layout(n_in);
     m->n = L.n;
     m->smem = (size_t)smem_layout(n_in).total;
-    m->infer_smem = (size_t)infer_smem(n_in).total;
+    m->tc_smem = (size_t)tc_smem(n_in, kTcWarps).total;
+    m->z0_smem = (size_t)tc_smem(n_in, 1).total;
     // seeded Glorot-uniform weights (SplitMix64 stream), zero biases
     std::vector<float> w(L.n, 0.0f);
     uint64_t st = seed;
@@ -594,7 +820,8 @@ int spdk_mlp_create(int n_in, int hidden, unsigned long long seed, spdk_mlp** ou
         cudaMalloc((void**)&m->m, L.n * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&m->v, L.n * sizeof(float)) != cudaSuccess ||
         cudaMalloc((void**)&m->g, L.n * sizeof(float)) != cudaSuccess ||
-        cudaMalloc((void**)&m->wbf, L.n * sizeof(uint16_t)) != cudaSuccess)
+        cudaMalloc((void**)&m->wbf, L.n * sizeof(uint16_t)) != cudaSuccess ||
+        cudaMalloc((void**)&m->z0, sizeof(float)) != cudaSuccess)
         rc = fail(SPDK_E_NOMEM, "mlp parameters");
     if (!rc) {
         cudaMemset(m->m, 0, L.n * sizeof(float));
@@ -604,10 +831,14 @@ int spdk_mlp_create(int n_in, int hidden, unsigned long long seed, spdk_mlp** ou
         if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem) !=
                 cudaSuccess ||
             cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->smem) != cudaSuccess ||
-            (m->infer_smem <= kInferSmemMax &&
-             cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->infer_smem) !=
-                 cudaSuccess))
+            cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->tc_smem) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_indicator_rows_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)m->tc_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_mlp_zero_logit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m->z0_smem) !=
+                cudaSuccess)
             rc = fail(SPDK_E_CUDA, "mlp shared memory request");
+        if (!rc) rc = update_zero_logit(m, 0);
         if (!rc && cudaDeviceSynchronize() != cudaSuccess) rc = fail(SPDK_E_CUDA, "mlp init");
     }
     if (rc) {
@@ -625,6 +856,7 @@ int spdk_mlp_destroy(spdk_mlp* m) {
     cudaFree(m->v);
     cudaFree(m->g);
     cudaFree(m->wbf);
+    cudaFree(m->z0);
     cudaFree(m->part);
     delete m;
     return 0;
@@ -651,6 +883,7 @@ int spdk_mlp_set_params(spdk_mlp* m, const float* host, int count) {
     cudaMemset(m->v, 0, count * sizeof(float));
     m->step = 0;
     k_to_bf16<<<grid_for(count, 256), 256>>>(m->w, m->wbf, count);
+    if (int rc = update_zero_logit(m, 0)) return rc;
     if (cudaDeviceSynchronize() != cudaSuccess) return fail(SPDK_E_CUDA, "mlp set_params");
     return 0;
 }
@@ -692,6 +925,7 @@ int spdk_mlp_train_step(spdk_mlp* m, const uint16_t* x, const float* y, const fl
     const float c2 = (float)(1.0 / (1.0 - std::pow(0.999, (double)m->step)));
     k_mlp_adam<<<grid_for(m->n, 256), 256, 0, (cudaStream_t)stream>>>(m->w, m->m, m->v, m->g, m->wbf, m->n, lr, c1,
                                                                      c2);
+    if (int rc2 = update_zero_logit(m, (cudaStream_t)stream)) return rc2;
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("mlp adam: ") + cudaGetErrorString(e));
 }

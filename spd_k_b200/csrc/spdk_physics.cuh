@@ -8,6 +8,8 @@
 // rho, m_1..m_D, E (V = D+2): in 2D the reference also carries m_z = 0,
 // whose terms only ever add or multiply signed zeros, so they are dropped.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <cstdint>
 
 namespace spdk {
@@ -169,16 +171,14 @@ __device__ __forceinline__ void hancock(const R* W, R* dWt, const R (*dW)[D + 2]
 }
 
 // src/trouble_detection.cpp:12-31 (smooth-extrema indicator)
+// (the reference divides both one-sided limits and then selects one; only
+// the selected quotient is formed here, which gives the same value)
 __device__ __forceinline__ double sed_alpha(double dv, double dUm, double dU, double dUp) {
-    double vL = dU - dUm;
-    double ap = smin(1.0, smax(vL, 0.0) / dv);
-    double am = smin(1.0, smin(vL, 0.0) / dv);
-    double aL = (dv < 0.0 ? am : ap);
+    const double vL = dU - dUm;
+    double aL = smin(1.0, (dv < 0.0 ? smin(vL, 0.0) : smax(vL, 0.0)) / dv);
     aL = (dv == 0.0 ? 1.0 : aL);
-    double vR = dUp - dU;
-    ap = smin(1.0, smax(vR, 0.0) / dv);
-    am = smin(1.0, smin(vR, 0.0) / dv);
-    double aR = (dv < 0.0 ? am : ap);
+    const double vR = dUp - dU;
+    double aR = smin(1.0, (dv < 0.0 ? smin(vR, 0.0) : smax(vR, 0.0)) / dv);
     aR = (dv == 0.0 ? 1.0 : aR);
     return smin(aL, aR);
 }
@@ -202,6 +202,38 @@ __device__ __forceinline__ int fv_image(int a, int n, int bc, bool* flip) {
 // correctly rounded result as the division)
 template <typename R> __device__ __forceinline__ R div_h(R x, R h, R rh, bool pow2) {
     return pow2 ? x * rh : x / h;
+}
+
+// ---------------------------------------------------------------------------
+// Feature values of the learned indicator, shared by the feature kernels and
+// the solver's update epilogue. Every FP64 operation is an explicitly
+// rounded intrinsic, so the values do not depend on the translation unit's
+// contraction flags (the FP32 form's units allow FMA).
+// ---------------------------------------------------------------------------
+// density and pressure of the state u[0], u[stride], ..., u[(V-1) stride]
+template <typename R>
+__device__ __forceinline__ void feature_rho_p(const R* u, int stride, int V, double gm, double* rho, double* p) {
+    const double r = (double)u[0];
+    double m2 = 0;
+    for (int d = 1; d < V - 1; d++) {
+        const double m = (double)u[d * stride];
+        m2 = __dadd_rn(m2, __dmul_rn(m, m));
+    }
+    *rho = r;
+    *p = __dmul_rn(__dsub_rn((double)u[(V - 1) * stride], __ddiv_rn(__dmul_rn(0.5, m2), r)), gm - 1.0);
+}
+
+// BF16 bit pattern of x, rounded to nearest even
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    const __nv_bfloat16 b = __float2bfloat16_rn(x);
+    return *reinterpret_cast<const uint16_t*>(&b);
+}
+
+// a / b - 1 (0 where b is not a positive finite number or the result is
+// not finite)
+__device__ __forceinline__ float feature_ratio(double a, double b) {
+    const double r = (b > 0 && isfinite(b)) ? __dsub_rn(__ddiv_rn(a, b), 1.0) : 0.0;
+    return isfinite(r) ? (float)r : 0.0f;
 }
 
 }  // namespace spdk

@@ -92,6 +92,54 @@ def test_gradient_matches_cpu_oracle():
     ind.close()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,N", [("fp64", 32), ("fp32", 32), ("fp64", 30), ("fp32", 30)])
+def test_solver_indicator_flags_match_oracle(precision, N):
+    """The solver's indicator builds the feature rows on chip and runs the
+    network on the tensor cores (one pass over 4 x 4 element tiles when the
+    element counts allow, else element means first); its flags equal the
+    restatement's features -> forward -> p > threshold except within 1e-5
+    of the threshold."""
+    from spd_k_b200.learned import Indicator, set_indicator
+    from spd_k_b200.api import FIELD_ELEMENT_PREDICTED
+    rng = np.random.default_rng(5)
+    g = blast(N, precision)
+    for _ in range(6):
+        g.step()
+    ind = Indicator(40, seed=2)
+    theta = rng.normal(0, 0.3, ind.n_params).astype(np.float32)
+    ind.set_params(theta)
+    u = g.read(0).reshape(g.info.n_elements, g.info.nvar, g.info.n_points)
+    X = MO.bits_to_float(MO.features(u, 2, g.p, list(g.N), [1, 1, 1], g.c["gamma"]))
+    p_ref, _ = MO.forward(MO.bf16_round(theta), X)
+    # the uniform background gives many elements one value: threshold in
+    # the middle of the distinct values
+    thr = float(np.median(np.unique(p_ref)))
+    set_indicator(g, ind, thr)
+    g.step()                                       # flags of the state before the step
+    pred = g.read(FIELD_ELEMENT_PREDICTED)
+    want = p_ref > thr
+    clear = np.abs(p_ref - thr) > 1e-5
+    assert 0 < want.sum() < len(want)
+    assert np.array_equal(pred[clear] > 0, want[clear])
+    # later steps take the features the previous step's last update stored,
+    # stepped one by one and by graph replay
+    for advance in (lambda: g.step(), lambda: g.steps(1)):
+        advance()
+        g.sync()
+        u = g.read(0).reshape(g.info.n_elements, g.info.nvar, g.info.n_points)
+        X = MO.bits_to_float(MO.features(u, 2, g.p, list(g.N), [1, 1, 1], g.c["gamma"]))
+        p_ref, _ = MO.forward(MO.bf16_round(theta), X)
+        advance()
+        g.sync()
+        pred = g.read(FIELD_ELEMENT_PREDICTED)
+        clear = np.abs(p_ref - thr) > 1e-5
+        assert np.array_equal(pred[clear] > 0, (p_ref > thr)[clear])
+    set_indicator(g, None)
+    g.close()
+    ind.close()
+
+
 def _rates(pred, lab):
     tp = float(np.sum((pred > 0) & (lab > 0)))
     fp = float(np.sum((pred > 0) & (lab == 0)))
