@@ -573,6 +573,8 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
     // SD face fluxes of the tile
     const int nfaces[3] = {SM::NF0, SM::NF1, SM::NF2};
     int fbase[3] = {0, SM::NF0, SM::NF0 + SM::NF1};
+    // direction loops unrolled: ffd, nfaces and fbase stay in registers
+#pragma unroll
     for (int d = 0; d < D; d++) {
         const int ex = Bx + (d == 0), ey = By + (d == 1);
         for (int q = threadIdx.x; q < nfaces[d]; q += blockDim.x) {
@@ -595,7 +597,9 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
     __syncthreads();
     // faces that blend in the fallback flux
     int need = 0;
-    for (int d = 0; d < D && !need; d++) {
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        if (need) break;
         const int ex = Bx + (d == 0), ey = By + (d == 1);
         for (int q = threadIdx.x; q < nfaces[d]; q += blockDim.x) {
             int a[3] = {q % ex, (q / ex) % ey, q / (ex * ey)};

@@ -359,8 +359,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // interior flux point of direction d: interpolation, primitives, Euler flux
 template <typename R, int D, int P, int TX, int TY, int TZ, int d>
-__device__ __forceinline__ void picard_interior_item(const DevGrid& G, const DevMatsT<R>& M, const R* Ss,
-                                                     R* FX, int q) {
+__device__ __forceinline__ void picard_interior_item(const DevGrid& G, const R* sp_to_fp, const R* Ss, R* FX, int q) {
     using S = Shape<D, P>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
     constexpr int NE = TX * TY * TZ;
@@ -378,7 +377,7 @@ __device__ __forceinline__ void picard_interior_item(const DevGrid& G, const Dev
 #pragma unroll
         for (int l = 0; l < n; l++) {
             c[d] = l;
-            a += src[v * NPT + pt_index<n>(c)] * M.sp_to_fp[ll * n + l];
+            a += src[v * NPT + pt_index<n>(c)] * sp_to_fp[ll * n + l];
         }
         u[v] = a;
     }
@@ -521,8 +520,19 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
     R* TT = FX0 + NFX * D * NE * V * FXS;  // [NE][V][NFP] face-integral scratch (3D)
     __shared__ long long sl_elem[NS];
     __shared__ uint64_t bar[2];
+    // the transform matrices in shared memory: the per-point coefficient
+    // lookups differ across a warp's lanes, which the constant bank (where
+    // the kernel parameters live) serves one address at a time
+    __shared__ R Msf[S::nf * S::n];   // sp_to_fp [nf][n]
+    __shared__ R Mdf[S::n * S::nf];   // dfp_to_sp [n][nf]
+    __shared__ R Mcv[S::n * S::n];    // sp_to_cv [n][n]
 
     const int tid = threadIdx.x;
+    for (int i = tid; i < S::nf * S::n; i += kThreads) {
+        Msf[i] = M.sp_to_fp[i];
+        Mdf[i] = M.dfp_to_sp[i];
+    }
+    for (int i = tid; i < S::n * S::n; i += kThreads) Mcv[i] = M.sp_to_cv[i];
     int o[3];
     {
         int b = bidx;
@@ -612,9 +622,9 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                 else if (D == 3 && q < NFT) picard_face_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
                 else {
                     const int r = q - NFT;
-                    if (r < NINT) picard_interior_item<R, D, P, TX, TY, TZ, 0>(G, M, Ss, FX, r);
-                    else if (r < 2 * NINT) picard_interior_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, r - NINT);
-                    else picard_interior_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, r - 2 * NINT);
+                    if (r < NINT) picard_interior_item<R, D, P, TX, TY, TZ, 0>(G, Msf, Ss, FX, r);
+                    else if (r < 2 * NINT) picard_interior_item<R, D, P, TX, TY, TZ, 1>(G, Msf, Ss, FX, r - NINT);
+                    else picard_interior_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, Msf, Ss, FX, r - 2 * NINT);
                 }
             };
             constexpr int TI = kThreads - NFT;  // threads left for the interior points
@@ -660,7 +670,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                             for (int ll = 0; ll < nf; ll++)
 #pragma unroll
                                 for (int d = 0; d < D; d++)
-                                    dudt += FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]] * M.dfp_to_sp[c[d] * nf + ll];
+                                    dudt += FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]] * Mdf[c[d] * nf + ll];
                             dudt *= (R)G.rh[0];
                         } else {
 #pragma unroll
@@ -668,7 +678,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
 #pragma unroll
                                 for (int d = 0; d < D; d++) {
                                     const R Fv = FX[((d * NE + el) * V + v) * FXS + fpi[d][ll]];
-                                    dudt += div_h(Fv * M.dfp_to_sp[c[d] * nf + ll], (R)G.h[d], (R)G.rh[d], G.pow2[d] != 0);
+                                    dudt += div_h(Fv * Mdf[c[d] * nf + ll], (R)G.h[d], (R)G.rh[d], G.pow2[d] != 0);
                                 }
                             }
                         }
@@ -844,7 +854,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
             const R* src = Wsp;
             for (int d = 0; d < D; d++) {
                 R* dst = bufs[d % 2];
-                sweep_smem<D, P, R>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+                sweep_smem<D, P, R>(src, dst, Mcv, d, NE * V * NPT);
                 __syncthreads();
                 src = dst;
             }
@@ -879,7 +889,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         const R* src = Ut;
         for (int d = 0; d < D; d++) {
             R* dst = bufs[d % 2];
-            sweep_smem<D, P, R>(src, dst, M.sp_to_cv, d, NE * V * NPT);
+            sweep_smem<D, P, R>(src, dst, Mcv, d, NE * V * NPT);
             __syncthreads();
             src = dst;
         }

@@ -462,12 +462,18 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
 
 __device__ __forceinline__ uint32_t pack_bf(uint16_t lo, uint16_t hi) { return (uint32_t)lo | ((uint32_t)hi << 16); }
 
-// x == bf(h) + bf(m) + bf(l) exactly (round-to-nearest residuals)
-__device__ __forceinline__ void split3(float x, uint16_t* h, uint16_t* m, uint16_t* l) {
-    *h = to_bf(x);
-    const float r1 = x - bf(*h);
-    *m = to_bf(r1);
-    *l = to_bf(r1 - bf(*m));
+// (x0, x1) == hi + mid + lo exactly, each term a packed BF16 pair (x0 in
+// the low half), round-to-nearest residuals
+__device__ __forceinline__ void split3x2(float x0, float x1, uint32_t* hi, uint32_t* mid, uint32_t* lo) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+    const float2 hf = __bfloat1622float2(h);
+    const float r0 = x0 - hf.x, r1 = x1 - hf.y;
+    const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+    const float2 mf = __bfloat1622float2(m);
+    const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - mf.x, r1 - mf.y);
+    *hi = *reinterpret_cast<const uint32_t*>(&h);
+    *mid = *reinterpret_cast<const uint32_t*>(&m);
+    *lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 // B fragments of W1 (k < n_in, zero beyond) and W2, and the FP32 vectors
@@ -545,12 +551,7 @@ __device__ __forceinline__ void mlp16_tc(const TcSmem& S, const unsigned char* s
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const float* hp = acc[2 * kc + (r >> 1)] + 2 * (r & 1);
-            uint16_t h0, m0, l0, h1, m1, l1;
-            split3(hp[0], &h0, &m0, &l0);
-            split3(hp[1], &h1, &m1, &l1);
-            ah[r] = pack_bf(h0, h1);
-            am[r] = pack_bf(m0, m1);
-            al[r] = pack_bf(l0, l1);
+            split3x2(hp[0], hp[1], &ah[r], &am[r], &al[r]);
         }
 #pragma unroll
         for (int nt = 0; nt < 8; nt++) {
@@ -575,17 +576,6 @@ __device__ __forceinline__ void mlp16_tc(const TcSmem& S, const unsigned char* s
     z1 += __shfl_xor_sync(0xffffffffu, z1, 2);
     z[0] = z0 + vec[3 * kH];
     z[1] = z1 + vec[3 * kH];
-}
-
-// true when the warp's 16 staged rows are all zero (columns < n_in)
-__device__ __forceinline__ bool tile_is_zero(const TcSmem& S, const uint16_t* Xs, int n_in) {
-    const int lane = threadIdx.x & 31;
-    bool nz = false;
-    for (int q = lane; q < 16 * n_in; q += 32) {
-        const int row = q / n_in, k = q - row * n_in;
-        nz |= Xs[row * S.ldx + k] != 0;
-    }
-    return !__any_sync(0xffffffffu, nz);
 }
 
 __device__ __forceinline__ void write_outputs(const float z[2], long long s0, long long batch, float* __restrict__ p,
@@ -621,13 +611,39 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_mlp_infer_tc(int n_in, const 
     const long long tiles = (batch + 15) / 16;
     for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles; tile += (long long)gridDim.x * kTcWarps) {
         const long long s0 = tile * 16;
-        for (int q = lane; q < 16 * n_in; q += 32) {
-            const int row = q / n_in, k = q - row * n_in;
-            Xs[row * S.ldx + k] = s0 + row < batch ? x[(s0 + row) * n_in + k] : (uint16_t)0;
+        // the tile's 16 x n_in inputs in memory order, four loads in
+        // flight per lane (row and column advanced without division); a
+        // tile of all-zero rows takes the zero-input logit
+        unsigned nz = 0;
+        const int total = 16 * n_in;
+        int row = lane / n_in, k = lane - row * n_in;
+        const int drow = 32 / n_in, dk = 32 - drow * n_in;
+        for (int q0 = 0; q0 < total; q0 += 128) {
+            uint16_t v[4];
+            int rr[4], kk[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                rr[i] = row;
+                kk[i] = k;
+                const bool ok = q0 + 32 * i + lane < total && s0 + row < batch;
+                v[i] = ok ? x[(s0 + row) * n_in + k] : (uint16_t)0;
+                row += drow;
+                k += dk;
+                if (k >= n_in) {
+                    k -= n_in;
+                    row++;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (q0 + 32 * i + lane < total) {
+                    Xs[rr[i] * S.ldx + kk[i]] = v[i];
+                    nz |= v[i];
+                }
         }
         __syncwarp();
         float z[2] = {zz, zz};
-        if (!tile_is_zero(S, Xs, n_in)) mlp16_tc(S, sm, Xs, z);
+        if (__any_sync(0xffffffffu, nz != 0)) mlp16_tc(S, sm, Xs, z);
         write_outputs(z, s0, batch, p, flags, thr);
         __syncwarp();  // the next tile overwrites Xs
     }
@@ -671,9 +687,21 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_indicator_rows_tc(const uint1
     const long long tiles = (F.E + 15) / 16;
     for (long long tile = (long long)blockIdx.x * kTcWarps + warp; tile < tiles; tile += (long long)gridDim.x * kTcWarps) {
         const long long e0 = tile * 16;
-        for (int q = lane; q < 16 * nod; q += 32) {
-            const int row = q / nod, k = q - row * nod;
-            Xs[row * S.ldx + k] = e0 + row < F.E ? feat[(e0 + row) * n_in + k] : (uint16_t)0;
+        // the nodal columns of the 16 rows: all loads issued, then stored
+        unsigned nz = 0;
+        for (int k0 = 0; k0 < nod; k0 += 32) {
+            const int k = k0 + lane;
+            uint16_t v[16];
+#pragma unroll
+            for (int row = 0; row < 16; row++)
+                v[row] = (k < nod && e0 + row < F.E) ? feat[(e0 + row) * n_in + k] : (uint16_t)0;
+            if (k < nod) {
+#pragma unroll
+                for (int row = 0; row < 16; row++) {
+                    Xs[row * S.ldx + k] = v[row];
+                    nz |= v[row];
+                }
+            }
         }
         for (int q = lane; q < 16 * F.D; q += 32) {
             const int row = q / F.D, d = q - row * F.D;
@@ -681,11 +709,14 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_indicator_rows_tc(const uint1
             uint16_t f[4] = {0, 0, 0, 0};
             if (e < F.E) neighbour_features(mean, F, e, d, f);
 #pragma unroll
-            for (int i = 0; i < 4; i++) Xs[row * S.ldx + nod + 4 * d + i] = f[i];
+            for (int i = 0; i < 4; i++) {
+                Xs[row * S.ldx + nod + 4 * d + i] = f[i];
+                nz |= f[i];
+            }
         }
         __syncwarp();
         float z[2] = {zz, zz};
-        if (!tile_is_zero(S, Xs, n_in)) mlp16_tc(S, sm, Xs, z);
+        if (__any_sync(0xffffffffu, nz != 0)) mlp16_tc(S, sm, Xs, z);
         write_outputs(z, e0, F.E, nullptr, flags, thr);
         __syncwarp();
     }
