@@ -35,7 +35,8 @@ enum {
     SPDK_E_ARG = -1,       /* invalid argument / unsupported configuration */
     SPDK_E_CUDA = -2,      /* CUDA runtime error (message in spdk_last_error) */
     SPDK_E_NOMEM = -3,     /* device allocation failed */
-    SPDK_E_STATE = -4      /* call out of order */
+    SPDK_E_STATE = -4,     /* call out of order */
+    SPDK_E_IO = -5         /* a file could not be read or written */
 };
 
 enum { SPDK_BC_PERIODIC = 0, SPDK_BC_GRADFREE = 1, SPDK_BC_REFLECTIVE = 2 };
@@ -135,7 +136,7 @@ enum {
     SPDK_KERNEL_CORRECT = 1,  /* corrector / RK stage + W_cv + dt */
     SPDK_KERNEL_FLUX = 2,     /* last Picard pass writing FV face fluxes */
     SPDK_KERNEL_DETECT = 3,   /* NAD/SED/PAD */
-    SPDK_KERNEL_THETA = 4,    /* theta blending */
+    SPDK_KERNEL_THETA = 4,    /* theta blending (computed inside the update kernel: no launches) */
     SPDK_KERNEL_UPDATE = 5,   /* fallback fluxes + FV update (+ W_cv, dt) */
     SPDK_KERNEL_OTHER = 6,    /* dt hand-over */
     SPDK_KERNEL_KINDS = 7
@@ -148,6 +149,38 @@ int spdk_hydro_profile(spdk_hydro* h, int n, double* ms, long long* launches);
  * SPDK_FIELD_U_SP recomputes W_cv and dt */
 int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count);
 int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count);
+
+/* Checkpoint / restart (no counterpart in the reference, whose runs start
+ * from the initial condition). A checkpoint file holds U_sp in the solver's
+ * own arithmetic (raw doubles or floats), the next step's dt as the device
+ * holds it (after any output clamping) and the caller's time_evolution
+ * bookkeeping; restoring it into a solver created from the same
+ * configuration and stepping on gives the same states, bit for bit, as the
+ * run that was never interrupted. Little-endian binary: a 256-byte header
+ * (magic "SPDKCKP1") and the state. */
+typedef struct spdk_checkpoint_info {
+    double t;             /* simulated time of the state */
+    double t_output;      /* the caller's next output time */
+    long long steps;      /* steps taken so far */
+    long long outputs;    /* output files written so far */
+} spdk_checkpoint_info;
+/* blocking: waits for the solver's stream, then writes the file */
+int spdk_hydro_checkpoint(spdk_hydro* h, const char* path, const spdk_checkpoint_info* info);
+/* asynchronous: snapshots the state on the solver's stream (device copy)
+ * and returns; a copy stream and a writer thread move it to the file while
+ * the caller keeps stepping. One checkpoint is in flight at a time (a second
+ * call first waits for the first); spdk_hydro_checkpoint_wait returns the
+ * status of the write, and destroy waits too. */
+int spdk_hydro_checkpoint_async(spdk_hydro* h, const char* path, const spdk_checkpoint_info* info);
+int spdk_hydro_checkpoint_wait(spdk_hydro* h);
+/* load a checkpoint (configuration checked against the solver's); fills
+ * info when not NULL */
+int spdk_hydro_restore(spdk_hydro* h, const char* path, spdk_checkpoint_info* info);
+/* read a checkpoint's header without a solver or a GPU: its bookkeeping,
+ * precision (SPDK_PRECISION_*), order, element counts and time-stepping
+ * (integrator, RK order); any output pointer may be NULL */
+int spdk_checkpoint_peek(const char* path, spdk_checkpoint_info* info, int* precision, int* p, int N[3],
+                         int* integrator, int* rk_order);
 
 /* Host-only set-up (no GPU needed).
  * spdk_build_matrices: the transform matrices of degree p, as the reference

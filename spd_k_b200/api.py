@@ -27,6 +27,7 @@ FIELD_ELEMENT_TROUBLES, FIELD_ELEMENT_PREDICTED = 4, 5
 # arithmetic of the solver: the plain FP64 form (bitwise the reference) or
 # the FP32 precision form (FP64 kept for pressure recovery, detector bounds, dt)
 PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS_BY_ID = {v: k for k, v in PRECISIONS.items()}
 
 # per-problem <problem> defaults (src/main.cpp:31-65):
 # amp, v1, v2, v3, d0, d1, p0, p1, radius, sigma, dir
@@ -76,6 +77,12 @@ class HydroInfo(ctypes.Structure):
     ]
 
 
+class CheckpointInfo(ctypes.Structure):
+    """spdk_checkpoint_info (include/spdk.h)"""
+    _fields_ = [("t", ctypes.c_double), ("t_output", ctypes.c_double), ("steps", ctypes.c_longlong),
+                ("outputs", ctypes.c_longlong)]
+
+
 EXPORTS = (
     "spdk_last_error", "spdk_abi_version", "spdk_hydro_create", "spdk_hydro_destroy",
     "spdk_hydro_get_info", "spdk_hydro_get_dt", "spdk_hydro_set_dt", "spdk_hydro_step",
@@ -114,6 +121,13 @@ def load_library(path=LIB_PATH):
                                   ctypes.c_size_t]
     L.spdk_hydro_write.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                    ctypes.c_size_t]
+    ci = ctypes.POINTER(CheckpointInfo)
+    L.spdk_hydro_checkpoint.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ci]
+    L.spdk_hydro_checkpoint_async.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ci]
+    L.spdk_hydro_checkpoint_wait.argtypes = [ctypes.c_void_p]
+    L.spdk_hydro_restore.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ci]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.spdk_checkpoint_peek.argtypes = [ctypes.c_char_p, ci, ip, ip, ip, ip, ip]
     _lib = L
     return L
 
@@ -121,6 +135,19 @@ def load_library(path=LIB_PATH):
 def _check(rc):
     if rc != 0:
         raise SpdkError(f"spdk error {rc}: {_lib.spdk_last_error().decode()}")
+
+
+def checkpoint_peek(path):
+    """spdk_checkpoint_peek: a checkpoint's header, without a solver or a GPU"""
+    L = load_library()
+    info = CheckpointInfo()
+    prec, p, integ, rk = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    N = (ctypes.c_int * 3)()
+    _check(L.spdk_checkpoint_peek(os.fsencode(path), ctypes.byref(info), ctypes.byref(prec), ctypes.byref(p), N,
+                                  ctypes.byref(integ), ctypes.byref(rk)))
+    return {"t": info.t, "t_output": info.t_output, "steps": info.steps, "outputs": info.outputs,
+            "precision": PRECISIONS_BY_ID.get(prec.value, prec.value), "p": p.value, "N": list(N),
+            "integrator": integ.value, "rk_order": rk.value}
 
 
 def parse_athinput(text):
@@ -307,6 +334,21 @@ class HydroSolver:
         a = out if out is not None else np.empty(count, dtype=np.float64)
         _check(_lib.spdk_hydro_read(self.h, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), count))
         return a
+
+    def checkpoint(self, path, t=0.0, t_output=0.0, steps=0, outputs=0, wait=True):
+        """spdk_hydro_checkpoint (wait=True) or spdk_hydro_checkpoint_async"""
+        info = CheckpointInfo(t, t_output, steps, outputs)
+        fn = _lib.spdk_hydro_checkpoint if wait else _lib.spdk_hydro_checkpoint_async
+        _check(fn(self.h, os.fsencode(path), ctypes.byref(info)))
+
+    def checkpoint_wait(self):
+        _check(_lib.spdk_hydro_checkpoint_wait(self.h))
+
+    def restore(self, path):
+        """spdk_hydro_restore; returns the stored bookkeeping as a dict"""
+        info = CheckpointInfo()
+        _check(_lib.spdk_hydro_restore(self.h, os.fsencode(path), ctypes.byref(info)))
+        return {"t": info.t, "t_output": info.t_output, "steps": info.steps, "outputs": info.outputs}
 
     def write_u(self, u):
         u = np.ascontiguousarray(u, dtype=np.float64).ravel()

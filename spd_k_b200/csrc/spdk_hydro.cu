@@ -247,6 +247,7 @@ int set_attributes(const KernelSetT<R>& ks) {
 }
 
 void release(spdk_hydro* h) {
+    checkpoint_release(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],

@@ -4,6 +4,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "spdk.h"
@@ -62,4 +64,17 @@ struct spdk_hydro {
     std::vector<cudaEvent_t> ev;
     std::vector<int> ev_kind;
     size_t ev_used = 0;
+    // asynchronous checkpoint (spdk_checkpoint.cu): a device snapshot of U
+    // and dt, its pinned host copy, the copy stream and the writer thread
+    unsigned char* ck_dev = nullptr;
+    unsigned char* ck_host = nullptr;
+    size_t ck_bytes = 0;
+    cudaStream_t ck_stream = nullptr;
+    cudaEvent_t ck_snap = nullptr, ck_done = nullptr;
+    std::thread* ck_thread = nullptr;
+    int ck_status = 0;
+    std::string ck_error;
 };
+
+// joins a pending checkpoint write and frees its buffers (spdk_checkpoint.cu)
+void checkpoint_release(spdk_hydro* h);

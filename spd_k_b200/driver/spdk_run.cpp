@@ -17,6 +17,11 @@
 //   X/Y/Z_N<N>p<p>_0.dat: FV face coordinates of each direction.
 // It prints the reference's "evolution:" line (steps, seconds, ms/step,
 // zone-cycles/s) with the evolution timed without output I/O.
+// Additions for hydro runs (no reference counterpart): output/checkpoint_dt
+// > 0 writes checkpoint_<step>.spdk (spdk_hydro_checkpoint_async) into the
+// output directory every checkpoint_dt of simulated time, and
+// job/restart=<file> resumes a run from one; the resumed run's states and
+// output files equal the uninterrupted run's.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -226,11 +231,27 @@ int run_hydro(const Params& P, int p, const int N[3], const double L[3], double 
                    f.data(), f.size());
         n_output++;
     };
-    if (outputs) write_outputs();
-
-    // time_evolution (src/hydro_ader.hpp:215-273)
+    // time_evolution (src/hydro_ader.hpp:215-273), optionally resumed from
+    // a checkpoint (job/restart) and writing checkpoints every
+    // output/checkpoint_dt of simulated time, asynchronously and without
+    // changing any dt, so a run and its restarts step identically
     double t = 0, dt = 0, t_output = dt_out, t_io = 0;
     long long steps = 0;
+    const std::string restart = P.str("job", "restart", "");
+    if (!restart.empty()) {
+        spdk_checkpoint_info ci{};
+        check(spdk_hydro_restore(h, restart.c_str(), &ci));
+        t = ci.t;
+        t_output = ci.t_output;
+        steps = ci.steps;
+        n_output = (int)ci.outputs;
+        std::printf("restarted from %s: t = %.17g, step %lld\n", restart.c_str(), t, steps);
+    } else if (outputs) {
+        write_outputs();
+    }
+    const double ckpt_dt = P.real("output", "checkpoint_dt", -1.0);
+    const std::string ckpt_dir = ckpt_dt > 0 ? out_dir() : "";
+    double t_ckpt = t + ckpt_dt;
     check(spdk_hydro_get_dt(h, &dt));
     const auto t0 = std::chrono::steady_clock::now();
     while (t < tlim) {
@@ -250,8 +271,15 @@ int run_hydro(const Params& P, int p, const int N[3], const double L[3], double 
                 check(spdk_hydro_set_dt(h, dt));
             }
         }
+        if (ckpt_dt > 0 && t >= t_ckpt && t < tlim) {
+            const spdk_checkpoint_info ci{t, t_output, steps, n_output};
+            check(spdk_hydro_checkpoint_async(h, (ckpt_dir + "checkpoint_" + std::to_string(steps) + ".spdk").c_str(),
+                                              &ci));
+            t_ckpt = t + ckpt_dt;
+        }
     }
     check(spdk_hydro_sync(h));
+    check(spdk_hydro_checkpoint_wait(h));
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - t_io;
     std::printf("\nevolution: %lld steps, %g s (%g ms/step), %g zone-cycles/s\n", steps, secs,
                 steps ? secs / steps * 1e3 : 0.0, secs > 0 ? (double)info.n_dof * steps / secs : 0.0);
