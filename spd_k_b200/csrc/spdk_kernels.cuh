@@ -509,12 +509,12 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
     extern __shared__ __align__(128) unsigned char smem_raw[];
     R* smem = reinterpret_cast<R*>(smem_raw);
     R* Sbuf = smem;                     // 2 x [NS][SS >= V*NPT] (R buffer)
-    // [kFxBuffers][D][NE][V][FXS >= NFP]: with two buffers (FP32) the
-    // predictor and the corrector alternate them between slices, so a
-    // slice's flux points can be written while slow threads still read the
-    // previous slice's (no end-of-slice barrier); the flux pass uses the
-    // first only. FP64 keeps one buffer: its occupancy is bound by shared
-    // memory, and the larger footprint cost more than the barrier saved.
+    // [kFxBuffers][D][NE][V][FXS >= NFP]: with two buffers (FP32) every
+    // pass alternates them between slices, so a slice's flux points can be
+    // written while slow threads still read the previous slice's (no
+    // end-of-slice barrier). FP64 keeps one buffer: its occupancy is bound
+    // by shared memory, and the larger footprint cost more than the barrier
+    // saved.
     constexpr int NFX = kFxBuffers<R>;
     R* FX0 = Sbuf + 2 * NS * SS;
     R* TT = FX0 + NFX * D * NE * V * FXS;  // [NE][V][NFP] face-integral scratch (3D)
@@ -595,7 +595,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         // ---- stage slice t (prefetch t+1 into the other buffer) ----
         const int b = multi ? (t & 1) : 0;
         R* Ss = Sbuf + b * NS * SS;
-        R* FX = FX0 + (NFX == 1 || MODE == kFlux ? 0 : (t & 1)) * (D * NE * V * FXS);
+        R* FX = FX0 + (NFX == 1 ? 0 : (t & 1)) * (D * NE * V * FXS);
         if (multi && t + 1 < nt) issue(t + 1, b ^ 1);
         if (t == 0 || multi) {
             if (kBulk) mbar_wait_bounded(&bar[b], multi ? ((t >> 1) & 1) : 0, G.status);
@@ -704,7 +704,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
             }
         } else {
             // ---- FV face fluxes of slice t (src/transforms.cpp:378-481) ----
-            const R* Mc = M.sp_to_cv;
+            const R* Mc = Mcv;
 #pragma unroll
             for (int d = 0; d < D; d++) {
                 R* out = A.ff[d];
@@ -772,8 +772,9 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         }
         // one FX buffer is reused by the next slice; the next slice's staging
         // overwrites this slice's buffer, which the corrector's gravity
-        // source still reads; the flux pass reuses FX
-        if (NFX == 1 || MODE == kFlux || (MODE == kCorrect && G.grav)) __syncthreads();
+        // source still reads (with two FX buffers the flux pass's face
+        // integral reads only this slice's FX, which the next slice leaves)
+        if (NFX == 1 || (MODE == kCorrect && G.grav)) __syncthreads();
     }
     __syncthreads();
 
