@@ -33,6 +33,41 @@ def _check(L, rc):
         raise SpdkError(f"spdk error {rc}: {L.spdk_last_error().decode()}")
 
 
+def problem_dof(c):
+    """solution points of a configuration dict (active elements x (p+1)^d)"""
+    n = c["p"] + 1
+    active = [N for N in c["N"] if N > 1]
+    e = 1
+    for N in active:
+        e *= N
+    return e * n ** len(active)
+
+
+def partition(configs, world):
+    """Greedy size-balanced split of independent problems across ranks
+    (longest processing time first: problems in decreasing DOF, each to the
+    rank with the least DOF so far, ties to the lower rank and the lower
+    index). Deterministic, so every rank computes the same split without a
+    collective; returns one list of problem indices per rank, each in
+    increasing order."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(configs)), key=lambda i: (-problem_dof(configs[i]), i))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += problem_dof(configs[i])
+    return [sorted(p) for p in parts]
+
+
+def shard(configs, rank, world):
+    """(indices, configurations) of this rank's part of the ensemble"""
+    idx = partition(configs, world)[rank]
+    return idx, [configs[i] for i in idx]
+
+
 class Batch:
     """Many independent 2D problems (configuration dicts) stepped together."""
 
