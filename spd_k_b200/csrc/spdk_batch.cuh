@@ -53,7 +53,7 @@ __device__ __forceinline__ const Item& batch_item(const Item* __restrict__ items
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
-__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>)
+__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>)
     picard_batched(const BatchItem<PicardArgsT<R>>* __restrict__ items, int n, DevMatsT<R> M) {
     long long b;
     const BatchItem<PicardArgsT<R>>& it = batch_item(items, n, &b);

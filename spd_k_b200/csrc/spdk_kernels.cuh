@@ -477,9 +477,14 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // registers a thread); for the FP32 form in 2D, whose per-point slices take
 // half the registers of FP64, 3 (85) at p <= 2 and 4 (64) at p = 3, where
 // the extra resident warps outweigh a few spilled registers (measured on
-// B200: 159 us against 178 us per predictor pass at 256^2)
-template <typename R, int D, int P>
-constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3) ? (P == 3 ? 4 : 3) : 2;
+// B200: 159 us against 178 us per predictor pass at 256^2). The flux pass
+// keeps no per-slice registers and takes one block more at p = 3 in 2D
+// (FP32 5 blocks: 159 against 167 us; FP64 3 blocks: 338 against 376 us);
+// the predictor and corrector spill heavily there.
+template <typename R, int D, int P, int MODE>
+constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
+                                       ? (P == 3 ? (MODE == kFlux ? 5 : 4) : 3)
+                                       : (MODE == kFlux && D == 2 && P == 3 ? 3 : 2);
 
 // flux-point buffers of a Picard pass (alternated between slices when 2)
 template <typename R>
@@ -912,7 +917,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
-__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
     picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(G, M, A, blockIdx.x);
 }
 
