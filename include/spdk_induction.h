@@ -40,6 +40,14 @@ typedef struct spdk_induction_config {
     double nad_tolerance;
     int nad_delta, nad_moore, sed;
     int device;
+    /* apply a fallback where the corrector detects troubles (no reference
+     * counterpart: the reference detects and stops there). Each slice's
+     * edges touching a troubled sub-cell take the first-order upwind EMF of
+     * the slice-start face averages instead of the high-order one, and the
+     * faces are updated again from the edges (constrained transport: the
+     * discrete divergence is unchanged). 0 = the reference's behaviour.
+     * Needs fallback = 1. */
+    int fallback_apply;
 } spdk_induction_config;
 
 typedef struct spdk_induction spdk_induction;

@@ -438,6 +438,39 @@ __global__ void k_ind_relax(FVa Tr, FVa Ax, FVa Ay, FVa Az, int mask, int use_se
     }
 }
 
+// Fallback EMF (no counterpart in the reference, whose corrector detects
+// troubles but applies no fallback): on every sub-cell edge of direction
+// dim that touches a troubled cell (the aggregate slot of the detection),
+// the first-order upwind EMF v1 b2 - v2 b1 of the slice-start face averages
+// replaces the high-order edge EMF; b2 (faces normal to dim2) is upwinded
+// along dim1 by v1, b1 (normal to dim1) along dim2 by v2, with the
+// reference's upwind() rule. Edge (K, J, I) is the low corner, in the two
+// directions other than dim, of cell (K, J, I); the loop covers the edges
+// the face update of the active cells reads. Edges without a troubled cell
+// keep their value bit for bit.
+__global__ void k_ind_fallback_emf(FVa E, FVa B1, FVa B2, FVa Tr, int dim, int fx, int fy, int fz) {
+    const int dim1 = choose(dim, 1, 2, 0), dim2 = choose(dim1, 1, 2, 0);
+    const int Mx = (dim == 0 ? fx - 3 : fx - 2) - kNGH + 1;
+    const int My = (dim == 1 ? fy - 3 : fy - 2) - kNGH + 1;
+    const int Mz = (dim == 2 ? fz - 3 : fz - 2) - kNGH + 1;
+    const int agg = Tr.e[0] - 1;
+    const int o1[3] = {dim1 == 0, dim1 == 1, dim1 == 2}, o2[3] = {dim2 == 0, dim2 == 1, dim2 == 2};
+    GRID_LOOP(o, (long long)Mz * My * Mx) {
+        const int I = kNGH + (int)(o % Mx), J = kNGH + (int)((o / Mx) % My), K = kNGH + (int)(o / Mx / My);
+        double tr = 0;
+        for (int s1 = 0; s1 < 2; s1++)
+            for (int s2 = 0; s2 < 2; s2++)
+                tr = smax(tr, Tr.at(agg, K - s1 * o1[2] - s2 * o2[2], J - s1 * o1[1] - s2 * o2[1],
+                                    I - s1 * o1[0] - s2 * o2[0]));
+        if (tr > 0) {
+            const double b2L = B2.at(0, K - o1[2], J - o1[1], I - o1[0]), b2R = B2.at(0, K, J, I);
+            const double b1L = B1.at(0, K - o2[2], J - o2[1], I - o2[0]), b1R = B1.at(0, K, J, I);
+            const double v1 = velocity(dim1), v2 = velocity(dim2);
+            E.at(0, K, J, I) = v1 * upwind(b2L, b2R, v1) - v2 * upwind(b1L, b1R, v2);
+        }
+    }
+}
+
 #undef GRID_LOOP
 
 // src/initial_conditions.cpp:235-249
@@ -620,13 +653,20 @@ int fv_update(spdk_induction* s) {
         for (int d = 0; d < 3; d++)
             k_edge_integral<<<blocks_for(s->Ecc[d].pts() * 2), kBlock, 0, st>>>(s->Ecc[d], s->Efv[d], s->sp_to_cv,
                                                                                s->n, t, d);
-        for (int d = 0; d < 3; d++) {
-            const int e1 = (d + 1) % 3, e2 = (d + 2) % 3;
-            const int dim1 = (d + 1) % 3, dim2 = (d + 2) % 3;
-            k_fv_update_B<<<blocks_for(s->Bcv[d].pts()), kBlock, 0, st>>>(s->Bnew[d], s->Bold[d], s->Bcv[d],
-                                                                         s->Efv[e1], s->Efv[e2], s->fvf[dim1],
-                                                                         s->fvf[dim2], s->wt, s->dt, t, d, 1);
-        }
+        // with the fallback applied, this update only forms B_new and
+        // B_old for the detection; the faces are written after the EMFs of
+        // troubled edges are replaced
+        const int apply = s->cfg.fallback_apply ? 1 : 0;
+        auto face_update = [&](int write) {
+            for (int d = 0; d < 3; d++) {
+                const int e1 = (d + 1) % 3, e2 = (d + 2) % 3;
+                const int dim1 = (d + 1) % 3, dim2 = (d + 2) % 3;
+                k_fv_update_B<<<blocks_for(s->Bcv[d].pts()), kBlock, 0, st>>>(s->Bnew[d], s->Bold[d], s->Bcv[d],
+                                                                             s->Efv[e1], s->Efv[e2], s->fvf[dim1],
+                                                                             s->fvf[dim2], s->wt, s->dt, t, d, write);
+            }
+        };
+        face_update(apply ? 0 : 1);
         k_B_cv_from_cf<<<blocks_for(s->Bcv[0].pts()), kBlock, 0, st>>>(s->Bn4, s->Bcv[0], s->Bcv[1], s->Bcv[2],
                                                                        s->fp_to_cv, s->nf);
         // apply_fv_boundaries (:614-643)
@@ -643,6 +683,18 @@ int fv_update(spdk_induction* s) {
                 k_ind_sed<<<blocks_for(U.cells()), kBlock, 0, st>>>(s->Bn4, s->alpha[d], s->fvc[d], s->fvf[d], d, mask);
         k_ind_relax<<<blocks_for(U.cells()), kBlock, 0, st>>>(s->troubles, s->alpha[0], s->alpha[1], s->alpha[2], mask,
                                                               use_sed ? 1 : 0);
+        if (apply) {
+            // upwind EMFs on the troubled edges (slice-start faces, ghosts
+            // filled above), then the face update from the blended edges
+            for (int d = 0; d < 3; d++) {
+                const int dim1 = (d + 1) % 3, dim2 = (d + 2) % 3;
+                const long long edges = (long long)s->Efv[d].cells();
+                k_ind_fallback_emf<<<blocks_for(edges), kBlock, 0, st>>>(s->Efv[d], s->Bold[dim1], s->Bold[dim2],
+                                                                        s->troubles, d, s->fvn[0], s->fvn[1],
+                                                                        s->fvn[2]);
+            }
+            face_update(1);
+        }
     }
     // Transform_to_sp
     for (int d = 0; d < 3; d++) transform_2d(s, s->Bcv[d], s->Bfp[d], s->Tfp[d], s->cv_to_sp, d);
@@ -696,6 +748,7 @@ int spdk_induction_create(const spdk_induction_config* cfg, spdk_induction** out
     *out = nullptr;
     const spdk_induction_config& c = *cfg;
     if (c.p < 1 || c.p > kMaxP) return fail(SPDK_E_ARG, "p must be in 1..7");
+    if (c.fallback_apply && !c.fallback) return fail(SPDK_E_ARG, "fallback_apply needs fallback = 1");
     for (int d = 0; d < 3; d++) {
         if (c.N[d] < 2) return fail(SPDK_E_ARG, "the induction solver needs three active directions (nx1, nx2, nx3 > 1)");
         if (c.bc[d] < 0 || c.bc[d] > 2) return fail(SPDK_E_ARG, "unknown boundary type");

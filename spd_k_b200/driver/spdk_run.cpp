@@ -21,7 +21,9 @@
 // > 0 writes checkpoint_<step>.spdk (spdk_hydro_checkpoint_async) into the
 // output directory every checkpoint_dt of simulated time, and
 // job/restart=<file> resumes a run from one; the resumed run's states and
-// output files equal the uninterrupted run's.
+// output files equal the uninterrupted run's. For induction runs,
+// fallback/apply=true applies the upwind-EMF fallback where the corrector
+// detects troubles (the reference only detects).
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -306,6 +308,7 @@ int run_induction(const Params& P, int p, const int N[3], const double L[3], dou
     c.nad_delta = P.str("fallback", "NAD", "relative") == "delta";
     c.nad_moore = P.str("fallback", "NAD_neighbors", "2nd") == "2nd";
     c.sed = P.boolean("fallback", "SED", true);
+    c.fallback_apply = P.boolean("fallback", "apply", false);  // no reference counterpart
     spdk_induction* s = nullptr;
     check(spdk_induction_create(&c, &s));
     const std::string dir = outputs ? out_dir() : "";

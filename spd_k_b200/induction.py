@@ -19,6 +19,7 @@ class InductionConfig(ctypes.Structure):
         ("integrator", ctypes.c_int), ("rk_order", ctypes.c_int), ("fallback", ctypes.c_int),
         ("cfl", ctypes.c_double), ("nu", ctypes.c_double), ("nad_tolerance", ctypes.c_double),
         ("nad_delta", ctypes.c_int), ("nad_moore", ctypes.c_int), ("sed", ctypes.c_int), ("device", ctypes.c_int),
+        ("fallback_apply", ctypes.c_int),
     ]
 
 
@@ -27,6 +28,8 @@ def induction_config_from_params(params):
     c = config_from_params(params)
     v = params.get("induction", {}).get("nu")
     c["nu"] = 0.0025 if v is None else float(v)
+    a = params.get("fallback", {}).get("apply")
+    c["fallback_apply"] = a is not None and a.strip().lower() in ("true", "1", "yes", "on")
     return c
 
 
@@ -49,6 +52,7 @@ def make_induction_config(c, device=0):
     o.nad_tolerance = c["nad_tolerance"]
     o.nad_delta, o.nad_moore, o.sed = int(c["nad_delta"]), int(c["nad_moore"]), int(c["sed"])
     o.device = device
+    o.fallback_apply = int(bool(c.get("fallback_apply", False)))
     return o
 
 

@@ -72,3 +72,57 @@ def test_divergence_free_and_field_loop_advected():
     assert e0 > 0 and abs(e1 - e0) / e0 < 0.2
     assert np.all(np.isfinite(b1))
     g.close()
+
+
+def _sd_divergence(g, p, N):
+    """max |div B| h / max |B| at the solution points of the active
+    elements, from the face fields and dfp_to_sp (spdk_build_matrices)"""
+    import ctypes
+    from spd_k_b200.api import load_library
+    from spd_k_b200.induction import FIELD_BX_FP, FIELD_BY_FP, FIELD_BZ_FP
+    L = load_library()
+    n, E = p + 1, N + 2
+    D = np.zeros(n * (n + 1))
+    L.spdk_build_matrices.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 6
+    assert L.spdk_build_matrices(p, 1, None, D.ctypes.data, None, None, None, None) == 0
+    D = D.reshape(n, n + 1)
+    bx = g.read(FIELD_BX_FP).reshape(E, E, E, n, n, n + 1)[1:-1, 1:-1, 1:-1]
+    by = g.read(FIELD_BY_FP).reshape(E, E, E, n, n + 1, n)[1:-1, 1:-1, 1:-1]
+    bz = g.read(FIELD_BZ_FP).reshape(E, E, E, n + 1, n, n)[1:-1, 1:-1, 1:-1]
+    h = g.c["L"][0] / N
+    d = (np.einsum("kjiabl,cl->kjiabc", bx, D) + np.einsum("kjialc,bl->kjiabc", by, D)
+         + np.einsum("kjilbc,al->kjiabc", bz, D)) / h
+    return float(np.abs(d).max() * h / max(np.abs(bx).max(), np.abs(by).max(), np.abs(bz).max()))
+
+
+def test_applied_fallback_keeps_div_b_and_limits_the_loop():
+    """fallback/apply (no reference counterpart: the reference only
+    detects): upwind EMFs on the edges of troubled sub-cells. Constrained
+    transport keeps div B at round-off; the field loop's peak |B|^2 stays
+    below the unlimited run's and the upwind edges dissipate |B|^2; the
+    applied run is deterministic. Off (the default) the golden tests above
+    hold byte for byte."""
+    from spd_k_b200.api import SpdkError, apply_overrides
+    from spd_k_b200.induction import FIELD_B2_CV, InductionSolver, induction_config_from_params
+    ov = CASES["ind_golden_n8"]["overrides"]
+    p, N, n = 3, 8, 4
+    res = {}
+    for apply in ("false", "true", "true"):
+        c = induction_config_from_params(apply_overrides({}, ov + [f"fallback/apply={apply}"]))
+        g = InductionSolver(c)
+        g.run(c["tlim"], c["output_dt"])
+        b2 = g.read(FIELD_B2_CV)
+        res.setdefault(apply, []).append((b2, _sd_divergence(g, p, N)))
+        g.close()
+    (off, div_off), = res["false"]
+    (on, div_on), (on2, _) = res["true"]
+    assert div_off < 1e-12 and div_on < 1e-12
+    assert np.array_equal(on, on2)
+    a = off.reshape(4, N + 2, N + 2, N + 2, n, n, n)[:, 1:-1, 1:-1, 1:-1]
+    b = on.reshape(4, N + 2, N + 2, N + 2, n, n, n)[:, 1:-1, 1:-1, 1:-1]
+    assert not np.array_equal(a, b)
+    assert b[3].max() < a[3].max()
+    assert b[3].sum() < a[3].sum()
+    with pytest.raises(SpdkError, match="fallback_apply"):
+        c = induction_config_from_params(apply_overrides({}, ov + ["fallback/apply=true", "job/fallback=false"]))
+        InductionSolver(c)
