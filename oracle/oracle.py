@@ -41,7 +41,7 @@ class OrcCfg(ctypes.Structure):
         ("p0", ctypes.c_double), ("p1", ctypes.c_double), ("radius", ctypes.c_double),
         ("sigma", ctypes.c_double), ("dir", ctypes.c_int),
         ("cx", ctypes.c_double), ("cy", ctypes.c_double), ("cz", ctypes.c_double),
-        ("q", ctypes.c_double * 16), ("seed", ctypes.c_ulonglong),
+        ("q", ctypes.c_double * 16), ("seed", ctypes.c_ulonglong), ("nu", ctypes.c_double), ("beta", ctypes.c_double),
     ]
 
 
@@ -134,6 +134,9 @@ def config_from_params(params):
     for name, d in zip(PP_NAMES, dflt):
         c[name] = g("problem", name, d, int if name == "dir" else float)
     c["cx"], c["cy"], c["cz"] = 0.5 * L[0], 0.5 * L[1], 0.5 * L[2]
+    # src/main.cpp:236-237: hydro/nu, hydro/beta = -2./3*nu by default
+    c["nu"] = g("hydro", "nu", 0.0)
+    c["beta"] = g("hydro", "beta", -2. / 3 * c["nu"])
     return c
 
 
@@ -163,6 +166,8 @@ def make_cfg(c):
     for i, v in enumerate(c.get("q", [])):
         o.q[i] = v
     o.seed = c.get("seed", 0)
+    o.nu = c.get("nu", 0.0)
+    o.beta = c.get("beta", -2. / 3 * o.nu)
     return o
 
 

@@ -263,6 +263,7 @@ struct orc {
     dim_t d[3];
     sd_t W_sp, U_sp, W_cv, U_cv, T_sweep, U0_sp, U_ader_sp;
     sd_t U_ader_fp[3], F_ader_fp[3], T_fp[3];
+    sd_t dU_sp[3];  /* viscous runs: gradients at the solution points (dUx/dUy/dUz_sp) */
     fv_t U_new, W_new, U_old, W_old, troubles, theta, theta_tmp, F[3], alpha[3];
 };
 
@@ -538,6 +539,12 @@ static double compute_dt(orc* s, const sd_t* W) {
         if (s->act[1]) { cmax += (fabs(*SD(W, 0, VY, k, j, i, kk, jj, ii)) + cs); dxmin = smin(dxmin, dy); }
         if (s->act[2]) { cmax += (fabs(*SD(W, 0, VZ, k, j, i, kk, jj, ii)) + cs); dxmin = smin(dxmin, dz); }
         double dtm = cfl * dxmin / cmax / px;
+        /* src/hydro.cpp:245-254: diffusion limit on the sub-cell grid */
+        if (s->c.nu > 0.0) {
+            double dx_sub = dxmin / px;
+            double dt_visc = 0.25 * cfl * dx_sub * dx_sub / s->c.nu;
+            dtm = dtm < dt_visc ? dtm : dt_visc;
+        }
         red = red < dtm ? red : dtm;
     }
     return red;
@@ -574,6 +581,11 @@ static void sd_boundaries(orc* s, const sd_t* U, int dim) {
 
 /* src/hydro.cpp:368-418: LLF at every element interface of direction D
  * (ghost rows included), written to both adjacent flux points */
+/* src/hydro.cpp:265-268 */
+static void riemann_wind(double* F, const double* UL, const double* UR, double wind) {
+    for (int v = 0; v < NV; v++) F[v] = 0.5 * (UR[v] + UL[v]) + wind * (UR[v] - UL[v]);
+}
+
 static void sd_riemann(orc* s, const sd_t* U, const sd_t* F, int D) {
     static const int V1[3] = {VX, VY, VZ}, V2[3] = {VY, VZ, VX}, V3[3] = {VZ, VX, VY};
     int Nx = U->Nx - (D == 0), Ny = U->Ny - (D == 1), Nz = U->Nz - (D == 2);
@@ -598,11 +610,115 @@ static void sd_riemann(orc* s, const sd_t* U, const sd_t* F, int D) {
                 *SD(F, t, v, kL, jL, iL, kkL, jjL, iiL) = f[v];
                 *SD(F, t, v, kR, jR, iR, kkR, jjR, iiR) = f[v];
             }
+            if (s->c.nu > 0.0) {
+                /* viscous: the interface state the diffusive terms use */
+                riemann_wind(f, uL, uR, 0.5);
+                for (int v = 0; v < NV; v++) {
+                    *SD(U, t, v, kL, jL, iL, kkL, jjL, iiL) = f[v];
+                    *SD(U, t, v, kR, jR, iR, kkR, jjR, iiR) = f[v];
+                }
+            }
         }
     }
 }
 
-/* src/hydro_ader.hpp:278-289 (inviscid): sp->fp, fluxes, ghost fill, LLF */
+/* src/hydro.cpp:420-455: F += the wind-weighted interface value of the
+ * viscous flux (arguments swapped as the reference passes them) */
+static void sd_rusanov(orc* s, const sd_t* U, const sd_t* F, int D) {
+    int Nx = U->Nx - (D == 0), Ny = U->Ny - (D == 1), Nz = U->Nz - (D == 2);
+    int px = D == 0 ? 1 : U->nx, py = D == 1 ? 1 : U->ny, pz = D == 2 ? 1 : U->nz;
+    int n = choose(D, U->nx, U->ny, U->nz);
+    for (int k = 0; k < Nz; k++) for (int j = 0; j < Ny; j++) for (int i = 0; i < Nx; i++)
+    for (int kk = 0; kk < pz; kk++) for (int jj = 0; jj < py; jj++) for (int ii = 0; ii < px; ii++) {
+        int l = choose(D, i, j, k);
+        int kL = D == 2 ? l : k, jL = D == 1 ? l : j, iL = D == 0 ? l : i;
+        int kR = D == 2 ? l + 1 : k, jR = D == 1 ? l + 1 : j, iR = D == 0 ? l + 1 : i;
+        int kkL = D == 2 ? n - 1 : kk, jjL = D == 1 ? n - 1 : jj, iiL = D == 0 ? n - 1 : ii;
+        int kkR = D == 2 ? 0 : kk, jjR = D == 1 ? 0 : jj, iiR = D == 0 ? 0 : ii;
+        for (int t = 0; t < U->nt; t++) {
+            double uL[NV], uR[NV], f[NV];
+            for (int v = 0; v < NV; v++) {
+                uL[v] = *SD(U, t, v, kR, jR, iR, kkR, jjR, iiR);
+                uR[v] = *SD(U, t, v, kL, jL, iL, kkL, jjL, iiL);
+            }
+            riemann_wind(f, uL, uR, -0.5);
+            for (int v = 0; v < NV; v++) {
+                *SD(F, t, v, kL, jL, iL, kkL, jjL, iiL) += f[v];
+                *SD(F, t, v, kR, jR, iR, kkR, jjR, iiR) += f[v];
+            }
+        }
+    }
+}
+
+/* src/hydro.cpp:457-490: dU = d/d(dim) of the flux-point values at the
+ * solution points of the active elements */
+static void compute_gradient(orc* s, const sd_t* U, const sd_t* dU, double h, int dim) {
+    int q = choose(dim, dU->nx, dU->ny, dU->nz);
+    int nfc = s->nf;
+    for (int k = s->ghost[2]; k < dU->Nz - s->ghost[2]; k++)
+    for (int j = s->ghost[1]; j < dU->Ny - s->ghost[1]; j++)
+    for (int i = s->ghost[0]; i < dU->Nx - s->ghost[0]; i++)
+    for (int kk = 0; kk < dU->nz; kk++) for (int jj = 0; jj < dU->ny; jj++) for (int ii = 0; ii < dU->nx; ii++)
+    for (int t = 0; t < dU->nt; t++) for (int var = 0; var < NV; var++) {
+        double du = 0;
+        int id = choose(dim, ii, jj, kk);
+        for (int ll = 0; ll < q + 1; ll++) {
+            double u = dim == 0 ? *SD(U, t, var, k, j, i, kk, jj, ll)
+                     : dim == 1 ? *SD(U, t, var, k, j, i, kk, ll, ii) : *SD(U, t, var, k, j, i, ll, jj, ii);
+            du += u * s->dfp_to_sp[id * nfc + ll] / h;
+        }
+        *SD(dU, t, var, k, j, i, kk, jj, ii) = du;
+    }
+}
+
+/* src/hydro.cpp:492-519 */
+static void viscous_fluxes(double* f, const double* w, const double* du1, int v1, const double* du2, int v2,
+                           const double* du3, int v3, double nu, double beta) {
+    f[0] = 0;
+    f[VP] = 0;
+    f[v1] = 2 * nu * du1[v1] + beta * du1[v1];
+    f[v1] += beta * du2[v2];
+    f[v2] = nu * (du1[v2] + du2[v1]);
+    f[VP] += w[v2] * f[v2];
+    f[v1] += beta * du3[v3];
+    f[v3] = nu * (du1[v3] + du3[v1]);
+    f[VP] += w[v3] * f[v3];
+    f[VP] += w[v1] * f[v1];
+}
+
+/* src/hydro.cpp:521-572: the viscous flux at every flux point of
+ * direction dim (ghost elements included), written over U */
+static void compute_viscous_flux(orc* s, const sd_t* U, const sd_t* dU1, int v1, const sd_t* dU2, int v2,
+                                 const sd_t* dU3, int v3, int dim) {
+    double nu = s->c.nu, beta = s->c.beta, gm = s->c.gamma;
+    int q = choose(dim, U->nx, U->ny, U->nz);
+    int n = s->n;
+    for (int k = 0; k < U->Nz; k++) for (int j = 0; j < U->Ny; j++) for (int i = 0; i < U->Nx; i++)
+    for (int kk = 0; kk < U->nz; kk++) for (int jj = 0; jj < U->ny; jj++) for (int ii = 0; ii < U->nx; ii++)
+    for (int t = 0; t < U->nt; t++) {
+        double f[NV] = {0}, u[NV], w[NV] = {0}, du1[NV], du2[NV], du3[NV];
+        int id = choose(dim, ii, jj, kk);
+        for (int var = 0; var < NV; var++) {
+            du1[var] = 0;
+            du2[var] = 0;
+            du3[var] = 0;
+            u[var] = *SD(U, t, var, k, j, i, kk, jj, ii);
+            for (int ll = 0; ll < q - 1; ll++) {
+                int nk = dim == 2 ? ll : kk, nj = dim == 1 ? ll : jj, ni = dim == 0 ? ll : ii;
+                du1[var] += *SD(dU1, t, var, k, j, i, nk, nj, ni) * s->sp_to_fp[id * n + ll];
+                du2[var] += *SD(dU2, t, var, k, j, i, nk, nj, ni) * s->sp_to_fp[id * n + ll];
+                du3[var] += *SD(dU3, t, var, k, j, i, nk, nj, ni) * s->sp_to_fp[id * n + ll];
+            }
+        }
+        primitives(u, w, gm);
+        viscous_fluxes(f, w, du1, v1, du2, v2, du3, v3, nu, beta);
+        for (int var = 0; var < NV; var++) *SD(U, t, var, k, j, i, kk, jj, ii) = f[var];
+    }
+}
+
+/* src/hydro_ader.hpp:278-289: sp->fp, fluxes, ghost fill, LLF; with
+ * hydro/nu > 0 the viscous terms (:380-405): gradients, viscous fluxes,
+ * ghost fill, interface sums */
 void orc_solve_fluxes(orc* s) {
     static const int V1[3] = {VX, VY, VZ}, V2[3] = {VY, VZ, VX}, V3[3] = {VZ, VX, VY};
     for (int d = 0; d < 3; d++)
@@ -613,6 +729,18 @@ void orc_solve_fluxes(orc* s) {
         if (s->act[d]) sd_boundaries(s, &s->U_ader_fp[d], d);
     for (int d = 0; d < 3; d++)
         if (s->act[d]) sd_riemann(s, &s->U_ader_fp[d], &s->F_ader_fp[d], d);
+    if (s->c.nu > 0.0) {
+        for (int d = 0; d < 3; d++)
+            if (s->act[d]) compute_gradient(s, &s->U_ader_fp[d], &s->dU_sp[d], s->d[d].h, d);
+        for (int d = 0; d < 3; d++)
+            if (s->act[d])
+                compute_viscous_flux(s, &s->U_ader_fp[d], &s->dU_sp[d], V1[d], &s->dU_sp[(d + 1) % 3], V2[d],
+                                     &s->dU_sp[(d + 2) % 3], V3[d], d);
+        for (int d = 0; d < 3; d++)
+            if (s->act[d]) sd_boundaries(s, &s->U_ader_fp[d], d);
+        for (int d = 0; d < 3; d++)
+            if (s->act[d]) sd_rusanov(s, &s->U_ader_fp[d], &s->F_ader_fp[d], d);
+    }
 }
 
 /* ------------------------------------------------------------------ */
@@ -1248,6 +1376,8 @@ orc* orc_create(const orc_cfg* cfg) {
     s->T_sweep = sd_alloc(1, NV, Nz, Ny, Nx, nz, ny, nx);
     s->U0_sp = sd_alloc(1, NV, Nz, Ny, Nx, nz, ny, nx);
     s->U_ader_sp = sd_alloc(s->nader, NV, Nz, Ny, Nx, nz, ny, nx);
+    if (cfg->nu > 0.0)
+        for (int d = 0; d < 3; d++) s->dU_sp[d] = sd_alloc(s->nader, NV, Nz, Ny, Nx, nz, ny, nx);
     for (int d = 0; d < 3; d++) {
         int fx = d == 0 && s->act[0], fy = d == 1 && s->act[1], fz = d == 2 && s->act[2];
         int ex = fx ? X->nfp : nx, ey = fy ? Y->nfp : ny, ez = fz ? Z->nfp : nz;
@@ -1277,7 +1407,8 @@ void orc_destroy(orc* s) {
     if (!s) return;
     sd_t* sds[] = {&s->W_sp, &s->U_sp, &s->W_cv, &s->U_cv, &s->T_sweep, &s->U0_sp, &s->U_ader_sp,
                    &s->U_ader_fp[0], &s->U_ader_fp[1], &s->U_ader_fp[2], &s->F_ader_fp[0], &s->F_ader_fp[1],
-                   &s->F_ader_fp[2], &s->T_fp[0], &s->T_fp[1], &s->T_fp[2]};
+                   &s->F_ader_fp[2], &s->T_fp[0], &s->T_fp[1], &s->T_fp[2], &s->dU_sp[0], &s->dU_sp[1],
+                   &s->dU_sp[2]};
     for (unsigned q = 0; q < sizeof(sds) / sizeof(sds[0]); q++) free(sds[q]->v);
     fv_t* fvs[] = {&s->U_new, &s->W_new, &s->U_old, &s->W_old, &s->troubles, &s->theta, &s->theta_tmp,
                    &s->F[0], &s->F[1], &s->F[2], &s->alpha[0], &s->alpha[1], &s->alpha[2]};

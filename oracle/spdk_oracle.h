@@ -47,6 +47,8 @@ typedef struct {
     /* extra problem parameters (project ICs) */
     double q[16];
     unsigned long long seed;
+    /* viscosity (src/main.cpp:236-243): hydro/nu, hydro/beta (default -2/3 nu) */
+    double nu, beta;
 } orc_cfg;
 
 typedef struct orc orc;

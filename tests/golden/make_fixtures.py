@@ -55,6 +55,18 @@ CASES = {
     "sod2d_p4": ["job/fallback=true", "mesh/p=4", "mesh/nx1=16", "mesh/nx2=2", "mesh/nx3=1",
                  "mesh/x1_bc=gradfree", "problem/problem=sod_shock_tube", "time/tlim=0.05", "output/dt=0.05"],
 }
+# viscous runs (hydro/nu > 0): the reference's viscous terms, served by the
+# prototype-level path (the fused solver rejects nu > 0)
+VISCOUS_CASES = {
+    "sine2d_viscous": ["job/fallback=false", "mesh/p=3", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1", "hydro/nu=0.01",
+                       "time/tlim=0.02", "output/dt=0.02"],
+    "kh2d_viscous_fallback": ["job/fallback=true", "mesh/p=2", "mesh/nx1=6", "mesh/nx2=6", "mesh/nx3=1",
+                              "hydro/nu=0.005", "problem/problem=kelvin_helmholtz", "time/tlim=0.02",
+                              "output/dt=0.02"],
+    "sine3d_viscous_rk2_beta": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=3",
+                                "hydro/nu=0.02", "hydro/beta=0.003", "time/integrator=rk2", "time/tlim=0.01",
+                                "output/dt=0.01"],
+}
 # full-size run of the plain-method CPU-runnable configuration (2D sine,
 # 32x32, p=3, ADER, LLF, to t=1): only rho and p are stored, with the
 # SHA-256 of the active rho, vx, vy, p slots
@@ -127,11 +139,10 @@ def sha256(path):
     return h.hexdigest()
 
 
-def main():
-    if not os.path.exists(REF_BIN):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
-    manifest = {"cases": {}, "goldens": {}}
-    for name, ov in CASES.items():
+def hydro_case(name, ov, entries):
+    """run the reference on one hydro case; W_cv of the last output (active
+    elements) into <name>.npz and its manifest entry into entries"""
+    if True:
         with tempfile.TemporaryDirectory() as out:
             env = dict(os.environ, SPD_OUTPUT_DIR=out, OMP_NUM_THREADS="8")
             r = subprocess.run([REF_BIN] + ov, capture_output=True, text=True, env=env, check=True)
@@ -151,10 +162,19 @@ def main():
             w = w[:, :, 1:-1, 1:-1]
             steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), W_cv=np.ascontiguousarray(w))
-            manifest["cases"][name] = {"overrides": ov, "output": last, "steps": steps,
-                                       "sha256": sha256(os.path.join(out, last)),
-                                       "shape": list(w.shape)}
+            entries[name] = {"overrides": ov, "output": last, "steps": steps,
+                             "sha256": sha256(os.path.join(out, last)), "shape": list(w.shape)}
             print(name, last, w.shape, steps, flush=True)
+
+
+def main():
+    if not os.path.exists(REF_BIN):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    manifest = {"cases": {}, "goldens": {}}
+    for name, ov in CASES.items():
+        hydro_case(name, ov, manifest["cases"])
+    for name, ov in VISCOUS_CASES.items():
+        hydro_case(name, ov, manifest.setdefault("viscous_cases", {}))
     for name, ov in FULL_CASES.items():
         with tempfile.TemporaryDirectory() as out:
             env = dict(os.environ, SPD_OUTPUT_DIR=out, OMP_NUM_THREADS="8")
@@ -201,7 +221,15 @@ def main():
 
 
 if __name__ == "__main__":
-    if "--induction" in sys.argv:
+    if "--viscous" in sys.argv:
+        # regenerate only the viscous fixtures, keeping the rest of the manifest
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            m = json.load(f)
+        for name, ov in VISCOUS_CASES.items():
+            hydro_case(name, ov, m.setdefault("viscous_cases", {}))
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(m, f, indent=1)
+    elif "--induction" in sys.argv:
         # regenerate only the induction fixtures, keeping the rest of the manifest
         with open(os.path.join(HERE, "manifest.json")) as f:
             m = json.load(f)

@@ -27,6 +27,18 @@ def test_oracle_reproduces_reference_fixture(case):
     assert sha256_bytes(reference_file_bytes(full)) == info["sha256"]
 
 
+@pytest.mark.parametrize("case", sorted(M.get("viscous_cases", {})))
+def test_oracle_reproduces_reference_viscous_fixture(case):
+    """hydro/nu > 0 (src/hydro.cpp:420-572: interface states, gradients,
+    viscous fluxes, interface sums; the diffusion dt limit), in 2D and 3D,
+    ADER and SSP-RK2, with and without the fallback, beta given or default"""
+    info = M["viscous_cases"][case]
+    w, steps, o, full = oracle_run(info["overrides"])
+    assert steps == info["steps"]
+    assert same_bits(w, fixture(case))
+    assert sha256_bytes(reference_file_bytes(full)) == info["sha256"]
+
+
 def test_oracle_reproduces_reference_golden_3d():
     """tests/goldens/hydro_sd/W_cv_N8p3_1_0.dat of the reference: 3D sine
     wave, N=8, p=3, ADER, t=0.1 (its run_tests.py hydro_sd_3d case)."""
