@@ -81,6 +81,9 @@ typedef struct spdk_hydro_config {
     unsigned long long seed;
     int precision;         /* SPDK_PRECISION_* */
     int device;            /* CUDA device ordinal */
+    double nu;             /* kinematic viscosity; > 0 switches the viscous terms on
+                              (hydro/nu, src/main.cpp:236; src/hydro.cpp:420-572) */
+    double beta;           /* bulk coefficient (hydro/beta, default -2/3 nu, src/main.cpp:237) */
 } spdk_hydro_config;
 
 typedef struct spdk_hydro spdk_hydro;

@@ -100,12 +100,32 @@ int spdk_fv_compute_primitives(const spdk_fv* u, const spdk_fv* w, const spdk_pr
 int spdk_compute_fluxes(const spdk_sd* u, const spdk_sd* f, int v1, int v2, int v3, const spdk_proto_cfg* cfg,
                         void* stream);
 /* src/prototypes.hpp:36 compute_dt(W, dx, dy, dz, nu): min over active points -> *dt_out (device);
- * nu must be 0 (the viscous terms are not on this path) */
+ * nu > 0 adds the diffusion limit 0.25 cfl (dx_min/(p+1))^2 / nu (src/hydro.cpp:245-254) */
 int spdk_compute_dt(const spdk_sd* w, double dx, double dy, double dz, double nu, double* dt_out,
                     const spdk_proto_cfg* cfg, void* stream);
-/* src/prototypes.hpp:55 sd_riemann_solver(U, F, v1, v2, v3, dim, viscous): LLF; viscous must be 0 */
+/* src/prototypes.hpp:54 sd_riemann_solver(U, F, v1, v2, v3, dim, viscous): LLF written to both
+ * interface flux points of F; viscous != 0 also writes the central interface state
+ * 0.5(uR+uL) + 0.5(uR-uL) over both interface points of U (src/hydro.cpp:370-413) */
 int spdk_sd_riemann_solver(const spdk_sd* u, const spdk_sd* f, int v1, int v2, int v3, int dim, int viscous,
                            const spdk_proto_cfg* cfg, void* stream);
+
+/* --- viscous terms (src/hydro.cpp:420-572), used when hydro/nu > 0 --------- */
+/* src/prototypes.hpp:55 sd_rusanov_solver(U, F, dim): F at both interface points +=
+ * 0.5(uR+uL) - 0.5(uR-uL) with uL = U at the right element's first flux point and
+ * uR = U at the left element's last (U holds viscous fluxes) */
+int spdk_sd_rusanov_solver(const spdk_sd* u, const spdk_sd* f, int dim, void* stream);
+/* src/prototypes.hpp:37 compute_gradient(U, dU, h, dfp_to_sp, dim): dU (solution points)
+ * = sum over the n+1 flux points along dim of U * dfp_to_sp / h, active elements only */
+int spdk_compute_gradient(const spdk_sd* u, const spdk_sd* du, double h, const spdk_mat* dfp_to_sp, int dim,
+                          const spdk_proto_cfg* cfg, void* stream);
+/* src/prototypes.hpp:38 compute_viscous_flux(U, dU1, v1, dU2, v2, dU3, v3, sp_to_fp, nu, beta, dim):
+ * at every flux point of direction dim (ghost elements included) the momentum
+ * gradients du1/du2/du3 interpolated along dim and the viscous flux
+ * (0, 2 nu du1 + beta div-part, nu (du1 + du2) ..., energy w.f) written over U;
+ * v1 = 1+dim, (v2, v3) the cyclic momentum slots */
+int spdk_compute_viscous_flux(const spdk_sd* u, const spdk_sd* du1, int v1, const spdk_sd* du2, int v2,
+                              const spdk_sd* du3, int v3, const spdk_mat* sp_to_fp, double nu, double beta, int dim,
+                              const spdk_proto_cfg* cfg, void* stream);
 
 /* --- boundaries (src/boundary.cpp) -------------------------------------- */
 /* src/prototypes.hpp:61 boundaries(comm, Boundaries{dim, type}, U): interface

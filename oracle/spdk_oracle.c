@@ -1486,6 +1486,9 @@ double* orc_array(orc* s, const char* name, int* dims) {
     FVN("troubles", s->troubles) FVN("theta", s->theta) FVN("U_new", s->U_new) FVN("U_old", s->U_old)
     FVN("W_new", s->W_new) FVN("W_old", s->W_old) FVN("F_x", s->F[0]) FVN("F_y", s->F[1]) FVN("F_z", s->F[2])
     FVN("alpha_x", s->alpha[0]) FVN("alpha_y", s->alpha[1]) FVN("alpha_z", s->alpha[2])
+    if (s->c.nu > 0.0) {
+        SDN("dUx_sp", s->dU_sp[0]) SDN("dUy_sp", s->dU_sp[1]) SDN("dUz_sp", s->dU_sp[2])
+    }
     int n = s->n, nf = s->nf;
     if (!strcmp(name, "sp_to_fp")) { fill_dims_1(nf, n, dims); return s->sp_to_fp; }
     if (!strcmp(name, "dfp_to_sp")) { fill_dims_1(n, nf, dims); return s->dfp_to_sp; }

@@ -65,6 +65,7 @@ class HydroConfig(ctypes.Structure):
         ("cx", ctypes.c_double), ("cy", ctypes.c_double), ("cz", ctypes.c_double),
         ("q", ctypes.c_double * 16), ("seed", ctypes.c_ulonglong),
         ("precision", ctypes.c_int), ("device", ctypes.c_int),
+        ("nu", ctypes.c_double), ("beta", ctypes.c_double),
     ]
 
 
@@ -212,6 +213,9 @@ def config_from_params(params):
     for name, d in zip(PP_NAMES, PROBLEM_DEFAULTS[problem]):
         c[name] = g("problem", name, d, int if name == "dir" else float)
     c["cx"], c["cy"], c["cz"] = 0.5 * L[0], 0.5 * L[1], 0.5 * L[2]
+    # src/main.cpp:236-237: viscosity is opt-in (hydro/nu > 0); beta = -2/3 nu by default
+    c["nu"] = g("hydro", "nu", 0.0)
+    c["beta"] = g("hydro", "beta", -2. / 3 * c["nu"])
     return c
 
 
@@ -247,6 +251,8 @@ def make_config(c, device=0):
         raise ValueError(f"unknown precision {prec!r} ({', '.join(PRECISIONS)})")
     o.precision = PRECISIONS[prec]
     o.device = device
+    o.nu = c.get("nu", 0.0)
+    o.beta = c.get("beta", -2. / 3 * o.nu)
     return o
 
 

@@ -314,6 +314,7 @@ int spdk_batch_create(const spdk_hydro_config* cfgs, int count, spdk_batch** out
             c.device != cfgs[0].device)
             return fail(SPDK_E_ARG, "all problems of a batch share precision, fallback and device");
         if (c.N[0] % 2 || c.N[1] % 2) return fail(SPDK_E_ARG, "element counts must be even");
+        if (c.nu != 0.0) return fail(SPDK_E_ARG, "the batched form is inviscid: set nu = 0");
     }
     spdk_batch* b = new spdk_batch;
     b->prec = cfgs[0].precision;

@@ -86,6 +86,22 @@ template <typename R>
 int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm) {
     const unsigned blocks = grid_blocks(h);
     int launches = 0;
+    // viscous face fluxes of a pass's input, written just before the pass
+    auto viscous = [&](PicardArgsT<R>& A) {
+        if (!h->vg[0]) return;
+        ViscArgsT<R> V{};
+        V.ua_in = A.ua_in;
+        V.in_slices = A.in_slices;
+        for (int d = 0; d < 3; d++) {
+            V.vg[d] = (R*)h->vg[d];
+            A.vg[d] = (const R*)h->vg[d];
+        }
+        const dim3 grid((unsigned)h->E, (unsigned)(A.in_slices > 1 ? h->nt : 1));
+        prof_begin(h);
+        k.visc<<<grid, kViscThreads, 0, h->stream>>>(h->G, dm, V);
+        prof_end(h, SPDK_KERNEL_OTHER);
+        launches++;
+    };
     R* const ua[2] = {(R*)h->ua[0], (R*)h->ua[1]};
     R* const ucv[2] = {(R*)h->ucv[0], (R*)h->ucv[1]};
     if (h->nstages > 1)
@@ -110,6 +126,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             A.ua_in = in;
             A.in_slices = in_slices;
             A.ua_out = ua[it % 2];
+            viscous(A);
             prof_begin(h);
             k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
             prof_end(h, SPDK_KERNEL_PREDICT);
@@ -119,6 +136,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
         }
         A.ua_in = in;
         A.in_slices = in_slices;
+        viscous(A);
         if (!h->cfg.fallback) {
             A.u_out = (R*)h->u;
             A.u0 = (const R*)h->u0;
@@ -181,7 +199,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
         }
     }
     prof_begin(h);
-    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
     prof_end(h, SPDK_KERNEL_OTHER);
     launches++;
     h->launches = launches;
@@ -253,7 +271,7 @@ void release(spdk_hydro* h) {
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
                     h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
                     h->rpo, h->rpn, h->trouble, h->theta, h->dtmin, h->status, h->elem_trouble, h->elem_pred,
-                    h->feat, h->means};
+                    h->feat, h->means, h->vg[0], h->vg[1], h->vg[2]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -285,6 +303,8 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         if (c.bc[d] < 0 || c.bc[d] > 2) return fail(SPDK_E_ARG, "bad boundary type");
     if (c.integrator == SPDK_INTEGRATOR_RK && (c.rk_order < 1 || c.rk_order > 3))
         return fail(SPDK_E_ARG, "rk_order must be 1, 2 or 3");
+    if (!(c.nu >= 0.0) || !std::isfinite(c.nu) || !std::isfinite(c.beta))
+        return fail(SPDK_E_ARG, "nu must be >= 0 and nu, beta finite");
 
     spdk_hydro* h = new spdk_hydro();
     h->cfg = c;
@@ -305,8 +325,9 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     int N[3] = {c.N[0], c.N[1], D == 3 ? c.N[2] : 1};
     h->prec = c.precision;
     h->esz = h->prec == SPDK_PRECISION_FP32 ? sizeof(float) : sizeof(double);
-    if (!select_kernels(D, c.p, N, &h->ks64) ||
-        (h->prec == SPDK_PRECISION_FP32 && !select_kernels(D, c.p, N, &h->ks32))) {
+    const bool visc = c.nu > 0.0;
+    if (!select_kernels(D, c.p, N, &h->ks64, visc) ||
+        (h->prec == SPDK_PRECISION_FP32 && !select_kernels(D, c.p, N, &h->ks32, visc))) {
         delete h;
         return fail(SPDK_E_ARG, "no kernel instantiation for this ndim/p");
     }
@@ -360,6 +381,16 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     G.nad_moore = c.nad_moore;
     G.use_sed = (c.sed && c.p > 1) ? 1 : 0;
     G.blending = c.blending;
+    G.nu = c.nu;
+    G.beta = c.beta;
+    if (c.nu > 0.0) {
+        // src/hydro.cpp:230-254: dx_min over the active directions (from 1),
+        // the diffusion limit 0.25 cfl (dx_min/(p+1))^2 / nu
+        double dxmin = 1;
+        for (int d = 0; d < D; d++) dxmin = G.h[d] < dxmin ? G.h[d] : dxmin;
+        const double dx_sub = dxmin / h->n;
+        h->dt_cap = 0.25 * c.cfl * dx_sub * dx_sub / c.nu;
+    }
 
     const size_t state = (size_t)h->E * h->V * h->NPT * h->esz;
     const size_t state64 = (size_t)h->E * h->V * h->NPT * sizeof(double);
@@ -407,6 +438,10 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
             rc = fail(SPDK_E_CUDA, "memset");
         if (!rc && cudaMemset(h->theta, 0, (size_t)h->E * h->NPT) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset");
     }
+    if (!rc && c.nu > 0.0) {
+        const size_t vgb = (size_t)h->nt * h->E * 2 * h->V * (h->NPT / h->n) * h->esz;
+        for (int d = 0; d < D && !rc; d++) rc = dalloc(h, &h->vg[d], vgb);
+    }
     if (!rc) rc = h->prec == SPDK_PRECISION_FP32 ? set_attributes(h->ks32) : set_attributes(h->ks64);
     if (!rc) {
         // initial condition on the host (transcendentals through the same
@@ -423,7 +458,7 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
             const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
             cudaMemcpy(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice);
             h->ks64.init<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm64, w64, u64, h->dtmin);
-            advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+            advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
             const long long nv = h->E * h->V * h->NPT;
             if (h->prec == SPDK_PRECISION_FP32) {
                 narrow_kernel<<<1024, 256, 0, h->stream>>>(u64, (float*)h->u, nv);
@@ -467,6 +502,7 @@ int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info) {
     info->n_time_slices = h->nt;
     int l = 0;
     for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 2 * h->nt : 1);
+    if (h->vg[0]) l += h->nstages * h->nt;  // a viscous pre-pass before every Picard pass
     info->launches_per_step = l + 1 + (h->mlp ? 2 : 0);
     info->device_bytes = h->bytes;
     return 0;
@@ -636,7 +672,7 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
         SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
         h->ks32.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm32, (const float*)h->u,
                                                                     (float*)h->wcv, h->dtmin);
-        advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+        advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
         SPDK_CUDA(cudaGetLastError());
         // the pageable staging vector must outlive the copy
         SPDK_CUDA(cudaStreamSynchronize(h->stream));
@@ -646,7 +682,7 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
     h->ks64.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm64, (const double*)h->u,
                                                                 (double*)h->wcv, h->dtmin);
-    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin);
+    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
     SPDK_CUDA(cudaGetLastError());
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
     return 0;

@@ -40,6 +40,10 @@ struct spdk_hydro {
     double2 *rpo = nullptr, *rpn = nullptr;
     uint8_t *trouble = nullptr, *theta = nullptr;
     unsigned long long* dtmin = nullptr;
+    // viscous runs: face viscous fluxes of the pass being evaluated, per
+    // direction, and the diffusion limit on dt (0: inviscid)
+    void* vg[3] = {nullptr, nullptr, nullptr};
+    double dt_cap = 0.0;
     int* status = nullptr;  // device-detected faults (kStatus* bits)
     // learned indicator: per-element labels, predictions, feature rows
     uint8_t *elem_trouble = nullptr, *elem_pred = nullptr;

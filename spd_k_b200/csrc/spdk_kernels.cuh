@@ -55,6 +55,8 @@ struct DevGrid {
     // fallback settings
     double nad_tol;
     int nad_delta, nad_moore, use_sed, blending;
+    // viscous terms (hydro/nu > 0; src/hydro.cpp:420-572)
+    double nu, beta;
     // learned indicator: per element, set when NAD/SED/PAD flags any of its
     // sub-cells in any slice of the step (NULL: not recorded), and the
     // a-priori prediction that counts all its sub-cells troubled (NULL: off)
@@ -81,6 +83,7 @@ struct PicardArgsT {
     unsigned long long* dtmin;  // kCorrect: next-dt reduction
     int final_stage;       // kCorrect: compute W_cv and dt
     const double* dt;      // device dt of this step
+    const R* vg[3];        // viscous face fluxes of this pass's input (NULL: inviscid)
 };
 using PicardArgs = PicardArgsT<double>;
 
@@ -393,9 +396,10 @@ __device__ __forceinline__ void picard_interior_item(const DevGrid& G, const R* 
 // element interface of direction d: both interface states, ghost image at a
 // non-periodic domain edge (src/boundary.cpp:48-113), LLF flux written to
 // the adjacent flux points of the tile's elements
-template <typename R, int D, int P, int TX, int TY, int TZ, int d>
+template <typename R, int D, int P, int TX, int TY, int TZ, int d, bool VISC>
 __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMatsT<R>& M, const R* Ss, R* FX,
-                                                 const int o[3], int q) {
+                                                 const int o[3], int q, const R* vg, const long long* sl_elem,
+                                                 int vt) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP;
@@ -457,6 +461,36 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
     }
     R F[V];
     riemann_llf<D>(F, uL, uR, d, (R)G.gm);
+    if constexpr (VISC) {
+        // viscous interface flux (src/hydro.cpp:420-455): the two sides'
+        // viscous fluxes from the pre-pass, the ghost side an image of the
+        // active side, combined with wind -0.5 and the sides swapped
+        R gL[V], gR[V];
+        if (!ghostL) {
+            const long long eL = sl_elem[TL::slot(lL[0], lL[1], lL[2])];
+            const R* g = vg + ((((long long)vt * G.E + eL) * 2 + 1) * V) * NTP + tp;
+#pragma unroll
+            for (int v = 0; v < V; v++) gL[v] = g[v * NTP];
+        }
+        if (!ghostR) {
+            const long long eR = sl_elem[TL::slot(lR[0], lR[1], lR[2])];
+            const R* g = vg + ((((long long)vt * G.E + eR) * 2 + 0) * V) * NTP + tp;
+#pragma unroll
+            for (int v = 0; v < V; v++) gR[v] = g[v * NTP];
+        }
+        if (ghostL) {
+#pragma unroll
+            for (int v = 0; v < V; v++) gL[v] = gR[v];
+            if (G.bc[d] == kReflective) gL[1 + d] = -gL[1 + d];
+        }
+        if (ghostR) {
+#pragma unroll
+            for (int v = 0; v < V; v++) gR[v] = gL[v];
+            if (G.bc[d] == kReflective) gR[1 + d] = -gR[1 + d];
+        }
+#pragma unroll
+        for (int v = 0; v < V; v++) F[v] += wind_mix(gR[v], gL[v], R(-0.5));
+    }
     if (fidx >= 1) {
         c[d] = nf - 1;
         const int fi = fp_index<n, nf>(d, c);
@@ -495,7 +529,7 @@ constexpr int kFxBuffers = sizeof(R) == 4 ? 2 : 1;
 // interfaces, flux divergence and the ADER predictor / corrector update,
 // fused so that only U_ader crosses HBM.
 // ---------------------------------------------------------------------------
-template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
+template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
 __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMatsT<R>& M, const PicardArgsT<R>& A, long long bidx) {
     using S = Shape<D, P>;
     using TL = Tile<D, TX, TY, TZ>;
@@ -622,9 +656,13 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
             constexpr int NFT = NF0 + NF1 + NF2;
             constexpr int total = NFT + D * NINT;
             auto item = [&](int q) {
-                if (q < NF0) picard_face_item<R, D, P, TX, TY, TZ, 0>(G, M, Ss, FX, o, q);
-                else if (q < NF0 + NF1) picard_face_item<R, D, P, TX, TY, TZ, 1>(G, M, Ss, FX, o, q - NF0);
-                else if (D == 3 && q < NFT) picard_face_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1)>(G, M, Ss, FX, o, q - NF0 - NF1);
+                const int vt = A.in_slices > 1 ? t : 0;
+                if (q < NF0) picard_face_item<R, D, P, TX, TY, TZ, 0, VISC>(G, M, Ss, FX, o, q, A.vg[0], sl_elem, vt);
+                else if (q < NF0 + NF1)
+                    picard_face_item<R, D, P, TX, TY, TZ, 1, VISC>(G, M, Ss, FX, o, q - NF0, A.vg[1], sl_elem, vt);
+                else if (D == 3 && q < NFT)
+                    picard_face_item<R, D, P, TX, TY, TZ, (D == 3 ? 2 : 1), VISC>(G, M, Ss, FX, o, q - NF0 - NF1,
+                                                                                   A.vg[D == 3 ? 2 : 1], sl_elem, vt);
                 else {
                     const int r = q - NFT;
                     if (r < NINT) picard_interior_item<R, D, P, TX, TY, TZ, 0>(G, Msf, Ss, FX, r);
@@ -916,9 +954,11 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
     }
 }
 
-template <typename R, int D, int P, int TX, int TY, int TZ, int MODE>
+// VISC: instantiation that adds the viscous interface fluxes (hydro/nu > 0);
+// the inviscid kernels carry none of that code
+template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
 __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
-    picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(G, M, A, blockIdx.x);
+    picard_kernel_body<R, D, P, TX, TY, TZ, MODE, VISC>(G, M, A, blockIdx.x);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>

@@ -6,6 +6,7 @@
 
 #include "spdk_fallback.cuh"
 #include "spdk_kernels.cuh"
+#include "spdk_viscous.cuh"
 
 namespace spdk {
 
@@ -82,9 +83,12 @@ __global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMatsT<R>
     block_min_dt(dtl, dtmin);
 }
 
-// next dt <- reduced minimum; re-arm the reduction
-static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin) {
-    *dt = __longlong_as_double((long long)*dtmin);
+// next dt <- reduced minimum, capped by the viscous diffusion limit when
+// cap > 0 (src/hydro.cpp:245-254: every point's candidate is min(dt, cap),
+// so the minimum over points is min(reduced, cap)); re-arm the reduction
+static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin, double cap) {
+    const double v = __longlong_as_double((long long)*dtmin);
+    *dt = (cap > 0.0 && !(v < cap)) ? cap : v;
     *dtmin = 0x7FEFFFFFFFFFFFFFULL;
 }
 
@@ -100,21 +104,23 @@ struct KernelSetT {
     void (*update)(DevGrid, DevMatsT<R>, FallbackArgsT<R>) = nullptr;
     void (*init)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
     void (*derive)(DevGrid, DevMatsT<R>, const R*, R*, unsigned long long*) = nullptr;
+    void (*visc)(DevGrid, DevMatsT<R>, ViscArgsT<R>) = nullptr;
     size_t picard_smem = 0, update_smem = 0;
     int tile[3] = {1, 1, 1};
 };
 using KernelSet = KernelSetT<double>;
 
-template <typename R, int D, int P, int TX, int TY, int TZ>
+template <typename R, int D, int P, int TX, int TY, int TZ, bool VISC = false>
 KernelSetT<R> make_set() {
     KernelSetT<R> k;
-    k.predict = picard_kernel<R, D, P, TX, TY, TZ, kPredict>;
-    k.correct = picard_kernel<R, D, P, TX, TY, TZ, kCorrect>;
-    k.flux = picard_kernel<R, D, P, TX, TY, TZ, kFlux>;
+    k.predict = picard_kernel<R, D, P, TX, TY, TZ, kPredict, VISC>;
+    k.correct = picard_kernel<R, D, P, TX, TY, TZ, kCorrect, VISC>;
+    k.flux = picard_kernel<R, D, P, TX, TY, TZ, kFlux, VISC>;
     k.detect = fv_detect_kernel<R, D, P, TX, TY, TZ>;
     k.update = fv_update_kernel<R, D, P, TX, TY, TZ>;
     k.init = init_state_kernel<R, D, P>;
     k.derive = derive_kernel<R, D, P>;
+    k.visc = visc_face_kernel<R, D, P>;
     k.picard_smem = picard_smem_bytes<R, D, P, TX, TY, TZ>();
     k.update_smem = UpdateSmem<R, D, P, TX, TY, TZ>::bytes;
     k.tile[0] = TX;
@@ -124,8 +130,10 @@ KernelSetT<R> make_set() {
 }
 
 // Tile choice: the largest instantiated tile that divides the element counts.
+// Viscous runs (visc) take the one-element tile with the viscous Picard passes.
 template <typename R, int P>
-bool pick2(int Nx, int Ny, KernelSetT<R>* k) {
+bool pick2(int Nx, int Ny, KernelSetT<R>* k, bool visc) {
+    if (visc) { *k = make_set<R, 2, P, 1, 1, 1, true>(); return true; }
     if constexpr (P <= 4) {
         if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<R, 2, P, 4, 4, 1>(); return true; }
     }
@@ -134,27 +142,28 @@ bool pick2(int Nx, int Ny, KernelSetT<R>* k) {
     return true;
 }
 template <typename R, int P>
-bool pick3(int, int, int, KernelSetT<R>* k) {
-    *k = make_set<R, 3, P, 1, 1, 1>();
+bool pick3(int, int, int, KernelSetT<R>* k, bool visc) {
+    if (visc) *k = make_set<R, 3, P, 1, 1, 1, true>();
+    else *k = make_set<R, 3, P, 1, 1, 1>();
     return true;
 }
 
 // per-translation-unit selectors (spdk_select_*.cu): the FP64 units are
 // compiled without FMA contraction (reference rounding), the FP32 units with it
-bool select_2d_low(int p, const int N[3], KernelSetT<double>* k);   // p = 1..3
-bool select_2d_high(int p, const int N[3], KernelSetT<double>* k);  // p = 4..7
-bool select_3d(int p, const int N[3], KernelSetT<double>* k);       // p = 1..5
-bool select_f32_2d(int p, const int N[3], KernelSetT<float>* k);    // p = 1..7
-bool select_f32_3d(int p, const int N[3], KernelSetT<float>* k);    // p = 1..5
+bool select_2d_low(int p, const int N[3], KernelSetT<double>* k, bool visc);   // p = 1..3
+bool select_2d_high(int p, const int N[3], KernelSetT<double>* k, bool visc);  // p = 4..7
+bool select_3d(int p, const int N[3], KernelSetT<double>* k, bool visc);       // p = 1..5
+bool select_f32_2d(int p, const int N[3], KernelSetT<float>* k, bool visc);    // p = 1..7
+bool select_f32_3d(int p, const int N[3], KernelSetT<float>* k, bool visc);    // p = 1..5
 
-inline bool select_kernels(int D, int p, const int N[3], KernelSetT<double>* k) {
-    if (D == 2) return p <= 3 ? select_2d_low(p, N, k) : select_2d_high(p, N, k);
-    if (D == 3) return select_3d(p, N, k);
+inline bool select_kernels(int D, int p, const int N[3], KernelSetT<double>* k, bool visc = false) {
+    if (D == 2) return p <= 3 ? select_2d_low(p, N, k, visc) : select_2d_high(p, N, k, visc);
+    if (D == 3) return select_3d(p, N, k, visc);
     return false;
 }
-inline bool select_kernels(int D, int p, const int N[3], KernelSetT<float>* k) {
-    if (D == 2) return select_f32_2d(p, N, k);
-    if (D == 3) return select_f32_3d(p, N, k);
+inline bool select_kernels(int D, int p, const int N[3], KernelSetT<float>* k, bool visc = false) {
+    if (D == 2) return select_f32_2d(p, N, k, visc);
+    if (D == 3) return select_f32_3d(p, N, k, visc);
     return false;
 }
 

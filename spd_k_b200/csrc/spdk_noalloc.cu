@@ -92,6 +92,7 @@ extern "C" int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const doubl
     if (!cfg || !u_in || !u_out || !dt_inout) return fail(SPDK_E_ARG, "null argument");
     const spdk_hydro_config& c = *cfg;
     if (c.fallback) return fail(SPDK_E_ARG, "the allocation-free step has no fallback: set fallback = 0");
+    if (c.nu != 0.0) return fail(SPDK_E_ARG, "the allocation-free step has no viscous terms: set nu = 0");
     if (c.p < 1 || c.p > kMaxP) return fail(SPDK_E_ARG, "p must be in 1..7");
     if (c.N[0] < 2 || c.N[1] < 2) return fail(SPDK_E_ARG, "x and y must be active (nx1, nx2 > 1)");
     if (c.precision != SPDK_PRECISION_FP64) return fail(SPDK_E_ARG, "unsupported precision");

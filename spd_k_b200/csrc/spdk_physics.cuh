@@ -205,6 +205,35 @@ template <typename R> __device__ __forceinline__ R div_h(R x, R h, R rh, bool po
 }
 
 // ---------------------------------------------------------------------------
+// Viscous terms (hydro/nu > 0)
+// ---------------------------------------------------------------------------
+// src/hydro.cpp:265-268: upwind-weighted mean of two interface values; the
+// interface state of the diffusive terms takes wind = +0.5, the interface
+// viscous flux wind = -0.5 with the two sides swapped
+template <typename R> __device__ __forceinline__ R wind_mix(R uL, R uR, R wind) {
+    return R(0.5) * (uR + uL) + wind * (uR - uL);
+}
+
+// src/hydro.cpp:492-519: viscous flux along momentum component a1 (0-based
+// x, y, z; a2, a3 the cyclic others) from the momentum gradients along a1
+// (du1), a2 (du2), a3 (du3) and the velocity w, all indexed by component
+// (a component of an inactive direction is zero). fm: momentum fluxes, fe:
+// energy flux; the density flux is zero. Operation order of the reference.
+template <typename R>
+__device__ __forceinline__ void viscous_flux(const R* du1, const R* du2, const R* du3, const R* w, int a1, int a2,
+                                             int a3, R nu, R beta, R* fm, R& fe) {
+    fe = 0;
+    fm[a1] = R(2) * nu * du1[a1] + beta * du1[a1];
+    fm[a1] += beta * du2[a2];
+    fm[a2] = nu * (du1[a2] + du2[a1]);
+    fe += w[a2] * fm[a2];
+    fm[a1] += beta * du3[a3];
+    fm[a3] = nu * (du1[a3] + du3[a1]);
+    fe += w[a3] * fm[a3];
+    fe += w[a1] * fm[a1];
+}
+
+// ---------------------------------------------------------------------------
 // Feature values of the learned indicator, shared by the feature kernels and
 // the solver's update epilogue. Every FP64 operation is an explicitly
 // rounded intrinsic, so the values do not depend on the translation unit's

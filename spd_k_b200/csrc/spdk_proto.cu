@@ -174,7 +174,7 @@ __global__ void k_pointwise(double* __restrict__ in, int in_nv, double* __restri
 // src/hydro.cpp:208-262 over active points; min via the ordered bit pattern
 // of positive doubles
 __global__ void k_dt_arm(unsigned long long* out) { *out = 0x7FEFFFFFFFFFFFFFULL; }
-__global__ void k_compute_dt(SDa W, double dx, double dy, double dz, Cfg C, unsigned long long* out) {
+__global__ void k_compute_dt(SDa W, double dx, double dy, double dz, double nu, Cfg C, unsigned long long* out) {
     const int gz = C.act[2], gy = C.act[1], gx = C.act[0];
     const int Nz = W.e[2] - 2 * gz, Ny = W.e[3] - 2 * gy, Nx = W.e[4] - 2 * gx;
     const long long n = (long long)Nz * Ny * Nx * W.e[5] * W.e[6] * W.e[7];
@@ -193,7 +193,13 @@ __global__ void k_compute_dt(SDa W, double dx, double dy, double dz, Cfg C, unsi
         if (C.act[0]) { cmax += (fabs(W.at(0, kVX, k, j, i, kk, jj, ii)) + cs); dxmin = smin(dxmin, dx); }
         if (C.act[1]) { cmax += (fabs(W.at(0, kVY, k, j, i, kk, jj, ii)) + cs); dxmin = smin(dxmin, dy); }
         if (C.act[2]) { cmax += (fabs(W.at(0, kVZ, k, j, i, kk, jj, ii)) + cs); dxmin = smin(dxmin, dz); }
-        const double dtm = C.cfl * dxmin / cmax / px;
+        double dtm = C.cfl * dxmin / cmax / px;
+        if (nu > 0.0) {
+            // src/hydro.cpp:245-254: diffusion limit on the sub-cell spacing
+            const double dx_sub = dxmin / px;
+            const double dt_visc = 0.25 * C.cfl * dx_sub * dx_sub / nu;
+            dtm = dtm < dt_visc ? dtm : dt_visc;
+        }
         red = red < dtm ? red : dtm;
     }
     for (int s = 16; s > 0; s >>= 1) red = smin(red, __shfl_xor_sync(0xffffffffu, red, s));
@@ -201,7 +207,7 @@ __global__ void k_compute_dt(SDa W, double dx, double dy, double dz, Cfg C, unsi
 }
 
 // ---- SD boundaries and Riemann solver: src/boundary.cpp:48-113, src/hydro.cpp:368-418
-__global__ void k_riemann(SDa U, SDa F, int D, int v1, double gm) {
+__global__ void k_riemann(SDa U, SDa F, int D, int v1, double gm, int viscous) {
     const int Nx = U.e[4] - (D == 0), Ny = U.e[3] - (D == 1), Nz = U.e[2] - (D == 2);
     const int px = D == 0 ? 1 : U.e[7], py = D == 1 ? 1 : U.e[6], pz = D == 2 ? 1 : U.e[5];
     const int n = choose(D, U.e[7], U.e[6], U.e[5]);
@@ -230,6 +236,109 @@ __global__ void k_riemann(SDa U, SDa F, int D, int v1, double gm) {
             F.at(t, v, kL, jL, iL, kkL, jjL, iiL) = f[v];
             F.at(t, v, kR, jR, iR, kkR, jjR, iiR) = f[v];
         }
+        if (viscous) {
+            // central interface state, read only by the diffusive terms
+            for (int v = 0; v < U.e[1]; v++) {
+                const double a = U.at(t, v, kL, jL, iL, kkL, jjL, iiL), b = U.at(t, v, kR, jR, iR, kkR, jjR, iiR);
+                const double m = wind_mix(a, b, 0.5);
+                U.at(t, v, kL, jL, iL, kkL, jjL, iiL) = m;
+                U.at(t, v, kR, jR, iR, kkR, jjR, iiR) = m;
+            }
+        }
+    }
+}
+
+// ---- viscous terms: src/hydro.cpp:420-572 --------------------------------
+// sd_rusanov_solver: F at both flux points of an interface += the
+// wind-weighted (-0.5) mean of the two sides' viscous fluxes, the right
+// element's value taken as the left state
+__global__ void k_rusanov(SDa U, SDa F, int D) {
+    const int Nx = U.e[4] - (D == 0), Ny = U.e[3] - (D == 1), Nz = U.e[2] - (D == 2);
+    const int px = D == 0 ? 1 : U.e[7], py = D == 1 ? 1 : U.e[6], pz = D == 2 ? 1 : U.e[5];
+    const int n = choose(D, U.e[7], U.e[6], U.e[5]);
+    const long long cnt = (long long)Nz * Ny * Nx * pz * py * px * U.e[0];
+    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < cnt; o += (long long)gridDim.x * blockDim.x) {
+        long long r = o;
+        const int t = (int)(r % U.e[0]); r /= U.e[0];
+        const int ii = (int)(r % px); r /= px;
+        const int jj = (int)(r % py); r /= py;
+        const int kk = (int)(r % pz); r /= pz;
+        const int i = (int)(r % Nx); r /= Nx;
+        const int j = (int)(r % Ny); r /= Ny;
+        const int k = (int)r;
+        const int l = choose(D, i, j, k);
+        const int kL = D == 2 ? l : k, jL = D == 1 ? l : j, iL = D == 0 ? l : i;
+        const int kR = D == 2 ? l + 1 : k, jR = D == 1 ? l + 1 : j, iR = D == 0 ? l + 1 : i;
+        const int kkL = D == 2 ? n - 1 : kk, jjL = D == 1 ? n - 1 : jj, iiL = D == 0 ? n - 1 : ii;
+        const int kkR = D == 2 ? 0 : kk, jjR = D == 1 ? 0 : jj, iiR = D == 0 ? 0 : ii;
+        for (int v = 0; v < U.e[1]; v++) {
+            const double a = U.at(t, v, kR, jR, iR, kkR, jjR, iiR), b = U.at(t, v, kL, jL, iL, kkL, jjL, iiL);
+            const double f = wind_mix(a, b, -0.5);
+            F.at(t, v, kL, jL, iL, kkL, jjL, iiL) += f;
+            F.at(t, v, kR, jR, iR, kkR, jjR, iiR) += f;
+        }
+    }
+}
+
+// compute_gradient: dU = d/d(dim) of the flux-point values at the solution
+// points of the active elements (one thread per output value)
+__global__ void k_gradient(SDa U, SDa dU, double h, const double* __restrict__ M, int nfc, int dim, Cfg C) {
+    const int gz = C.act[2], gy = C.act[1], gx = C.act[0];
+    const int Nz = dU.e[2] - 2 * gz, Ny = dU.e[3] - 2 * gy, Nx = dU.e[4] - 2 * gx;
+    const long long cnt = (long long)Nz * Ny * Nx * dU.e[5] * dU.e[6] * dU.e[7] * dU.e[0] * dU.e[1];
+    const int q = choose(dim, dU.e[7], dU.e[6], dU.e[5]);
+    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < cnt; o += (long long)gridDim.x * blockDim.x) {
+        long long r = o;
+        const int var = (int)(r % dU.e[1]); r /= dU.e[1];
+        const int t = (int)(r % dU.e[0]); r /= dU.e[0];
+        const int ii = (int)(r % dU.e[7]); r /= dU.e[7];
+        const int jj = (int)(r % dU.e[6]); r /= dU.e[6];
+        const int kk = (int)(r % dU.e[5]); r /= dU.e[5];
+        const int i = gx + (int)(r % Nx); r /= Nx;
+        const int j = gy + (int)(r % Ny); r /= Ny;
+        const int k = gz + (int)r;
+        const int id = choose(dim, ii, jj, kk);
+        double du = 0;
+        for (int ll = 0; ll < q + 1; ll++) {
+            const double u = dim == 0 ? U.at(t, var, k, j, i, kk, jj, ll)
+                           : dim == 1 ? U.at(t, var, k, j, i, kk, ll, ii) : U.at(t, var, k, j, i, ll, jj, ii);
+            du += u * M[id * nfc + ll] / h;
+        }
+        dU.at(t, var, k, j, i, kk, jj, ii) = du;
+    }
+}
+
+// compute_viscous_flux: the gradients interpolated to every flux point of
+// direction dim (ghost elements included), the viscous flux written over U
+__global__ void k_viscous_flux(SDa U, SDa dU1, SDa dU2, SDa dU3, int v1, int v2, int v3,
+                               const double* __restrict__ M, int mcols, double nu, double beta, int dim, double gm) {
+    const int q = choose(dim, U.e[7], U.e[6], U.e[5]);
+    const long long cnt = U.pts() * U.e[0];
+    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < cnt; o += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)(o % U.e[0]);
+        int c[6];
+        point_of(U, o / U.e[0], c);
+        const int k = c[0], j = c[1], i = c[2], kk = c[3], jj = c[4], ii = c[5];
+        const int id = choose(dim, ii, jj, kk);
+        // momentum gradients by component (slot - 1) and the velocities
+        double du1[3], du2[3], du3[3], w[3];
+        for (int a = 0; a < 3; a++) {
+            du1[a] = 0;
+            du2[a] = 0;
+            du3[a] = 0;
+            for (int ll = 0; ll < q - 1; ll++) {
+                const int nk = dim == 2 ? ll : kk, nj = dim == 1 ? ll : jj, ni = dim == 0 ? ll : ii;
+                du1[a] += dU1.at(t, 1 + a, k, j, i, nk, nj, ni) * M[id * mcols + ll];
+                du2[a] += dU2.at(t, 1 + a, k, j, i, nk, nj, ni) * M[id * mcols + ll];
+                du3[a] += dU3.at(t, 1 + a, k, j, i, nk, nj, ni) * M[id * mcols + ll];
+            }
+        }
+        const double rho = U.at(t, 0, k, j, i, kk, jj, ii);
+        for (int a = 0; a < 3; a++) w[a] = U.at(t, 1 + a, k, j, i, kk, jj, ii) / rho;
+        double fm[3], fe;
+        viscous_flux(du1, du2, du3, w, v1 - 1, v2 - 1, v3 - 1, nu, beta, fm, fe);
+        for (int v = 0; v < U.e[1]; v++)
+            U.at(t, v, k, j, i, kk, jj, ii) = (v >= 1 && v <= 3) ? fm[v - 1] : (v == kVP ? fe : 0.0);
     }
 }
 
@@ -706,12 +815,12 @@ int spdk_compute_fluxes(const spdk_sd* u, const spdk_sd* f, int v1, int v2, int 
 int spdk_compute_dt(const spdk_sd* w, double dx, double dy, double dz, double nu, double* dt_out,
                     const spdk_proto_cfg* cfg, void* stream) {
     if (!cfg || !ok_sd(w) || !dt_out || w->ext[1] < kNV) return fail(SPDK_E_ARG, "compute_dt: bad argument");
-    if (nu != 0.0) return fail(SPDK_E_ARG, "compute_dt: viscous limit (nu > 0) is not supported");
+    if (!(nu >= 0.0)) return fail(SPDK_E_ARG, "compute_dt: nu must be >= 0");
     SDa W = sd(w);
     cudaStream_t s = (cudaStream_t)stream;
     unsigned long long* out = reinterpret_cast<unsigned long long*>(dt_out);
     k_dt_arm<<<1, 1, 0, s>>>(out);
-    k_compute_dt<<<blocks_for(W.pts()), kBlock, 0, s>>>(W, dx, dy, dz, cfgof(cfg), out);
+    k_compute_dt<<<blocks_for(W.pts()), kBlock, 0, s>>>(W, dx, dy, dz, nu, cfgof(cfg), out);
     return launched("compute_dt");
 }
 
@@ -719,13 +828,66 @@ int spdk_sd_riemann_solver(const spdk_sd* u, const spdk_sd* f, int v1, int v2, i
                            const spdk_proto_cfg* cfg, void* stream) {
     if (!cfg || !ok_sd(u) || !ok_sd(f) || dim < 0 || dim > 2 || u->ext[1] < kNV)
         return fail(SPDK_E_ARG, "sd_riemann_solver: bad argument");
-    if (viscous) return fail(SPDK_E_ARG, "sd_riemann_solver: viscous fluxes are not supported");
     if (v1 != 1 + dim || v2 < 1 || v2 > 3 || v3 < 1 || v3 > 3 || v2 == v3 || v2 == v1 || v3 == v1)
         return fail(SPDK_E_ARG, "sd_riemann_solver: v1 must be the normal momentum slot 1+dim");
     SDa U = sd(u);
     const long long n = U.pts() * U.e[0];
-    k_riemann<<<blocks_for(n), kBlock, 0, (cudaStream_t)stream>>>(U, sd(f), dim, v1, cfg->gamma);
+    k_riemann<<<blocks_for(n), kBlock, 0, (cudaStream_t)stream>>>(U, sd(f), dim, v1, cfg->gamma, viscous ? 1 : 0);
     return launched("sd_riemann_solver");
+}
+
+int spdk_sd_rusanov_solver(const spdk_sd* u, const spdk_sd* f, int dim, void* stream) {
+    if (!ok_sd(u) || !ok_sd(f) || dim < 0 || dim > 2 || u->ext[1] != f->ext[1] || u->ext[0] != f->ext[0])
+        return fail(SPDK_E_ARG, "sd_rusanov_solver: bad argument");
+    for (int q = 2; q < 8; q++)
+        if (u->ext[q] != f->ext[q]) return fail(SPDK_E_ARG, "sd_rusanov_solver: U and F extents differ");
+    if (choose(dim, u->ext[4], u->ext[3], u->ext[2]) < 2)
+        return fail(SPDK_E_ARG, "sd_rusanov_solver: direction has no interfaces");
+    SDa U = sd(u);
+    k_rusanov<<<blocks_for(U.pts() * U.e[0]), kBlock, 0, (cudaStream_t)stream>>>(U, sd(f), dim);
+    return launched("sd_rusanov_solver");
+}
+
+int spdk_compute_gradient(const spdk_sd* u, const spdk_sd* du, double h, const spdk_mat* dfp_to_sp, int dim,
+                          const spdk_proto_cfg* cfg, void* stream) {
+    if (!cfg || !ok_sd(u) || !ok_sd(du) || !ok_mat(dfp_to_sp) || dim < 0 || dim > 2 || !(h > 0.0))
+        return fail(SPDK_E_ARG, "compute_gradient: bad argument");
+    const int n = choose(dim, du->ext[7], du->ext[6], du->ext[5]);
+    if (choose(dim, u->ext[7], u->ext[6], u->ext[5]) != n + 1 || dfp_to_sp->rows < n || dfp_to_sp->cols != n + 1 ||
+        u->ext[0] != du->ext[0] || u->ext[1] < du->ext[1])
+        return fail(SPDK_E_ARG, "compute_gradient: U must hold n+1 flux points along dim for the n solution points of dU");
+    for (int q = 2; q < 5; q++)
+        if (u->ext[q] != du->ext[q]) return fail(SPDK_E_ARG, "compute_gradient: element extents differ");
+    SDa dU = sd(du);
+    k_gradient<<<blocks_for(dU.pts() * dU.e[0] * dU.e[1]), kBlock, 0, (cudaStream_t)stream>>>(
+        sd(u), dU, h, dfp_to_sp->data, dfp_to_sp->cols, dim, cfgof(cfg));
+    return launched("compute_gradient");
+}
+
+int spdk_compute_viscous_flux(const spdk_sd* u, const spdk_sd* du1, int v1, const spdk_sd* du2, int v2,
+                              const spdk_sd* du3, int v3, const spdk_mat* sp_to_fp, double nu, double beta, int dim,
+                              const spdk_proto_cfg* cfg, void* stream) {
+    if (!cfg || !ok_sd(u) || !ok_sd(du1) || !ok_sd(du2) || !ok_sd(du3) || !ok_mat(sp_to_fp) || dim < 0 || dim > 2 ||
+        u->ext[1] < kNV)
+        return fail(SPDK_E_ARG, "compute_viscous_flux: bad argument");
+    if (v1 != 1 + dim || v2 < 1 || v2 > 3 || v3 < 1 || v3 > 3 || v2 == v3 || v2 == v1 || v3 == v1)
+        return fail(SPDK_E_ARG, "compute_viscous_flux: v1 must be the normal momentum slot 1+dim");
+    const int n = choose(dim, du1->ext[7], du1->ext[6], du1->ext[5]);
+    if (choose(dim, u->ext[7], u->ext[6], u->ext[5]) != n + 1 || sp_to_fp->cols != n || sp_to_fp->rows < n + 1)
+        return fail(SPDK_E_ARG, "compute_viscous_flux: U must hold n+1 flux points along dim");
+    const spdk_sd* g[3] = {du1, du2, du3};
+    for (int a = 0; a < 3; a++) {
+        if (g[a]->ext[0] != u->ext[0] || g[a]->ext[1] < 4) return fail(SPDK_E_ARG, "compute_viscous_flux: gradient extents");
+        for (int q = 2; q < 8; q++) {
+            const bool along = (q == 7 && dim == 0) || (q == 6 && dim == 1) || (q == 5 && dim == 2);
+            if (!along && g[a]->ext[q] != u->ext[q])
+                return fail(SPDK_E_ARG, "compute_viscous_flux: gradient extents differ from U");
+        }
+    }
+    SDa U = sd(u);
+    k_viscous_flux<<<blocks_for(U.pts() * U.e[0]), kBlock, 0, (cudaStream_t)stream>>>(
+        U, sd(du1), sd(du2), sd(du3), v1, v2, v3, sp_to_fp->data, sp_to_fp->cols, nu, beta, dim, cfg->gamma);
+    return launched("compute_viscous_flux");
 }
 
 int spdk_boundaries_sd(const spdk_sd* u, int dim, int type, void* stream) {

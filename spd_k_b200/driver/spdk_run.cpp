@@ -177,7 +177,10 @@ int run_hydro(const Params& P, int p, const int N[3], const double L[3], double 
     c.nad_moore = P.str("fallback", "NAD_neighbors", "2nd") == "2nd";
     c.sed = P.boolean("fallback", "SED", true);
     c.blending = P.boolean("fallback", "blending", true);
-    if (P.real("hydro", "nu", 0.0) > 0.0) throw std::runtime_error("viscous terms (hydro/nu > 0) are not supported");
+    // src/main.cpp:233-240: viscosity is opt-in (hydro/nu > 0), beta = -2/3 nu by default
+    c.nu = P.real("hydro", "nu", 0.0);
+    c.beta = P.real("hydro", "beta", -2. / 3 * c.nu);
+    if (c.nu > 0.0) std::cout << "viscosity on: nu = " << c.nu << ", beta = " << c.beta << std::endl;
     const std::string prob = P.str("problem", "problem", "sine_wave");
     const Problem* pr = nullptr;
     for (const Problem& q : kProblems)

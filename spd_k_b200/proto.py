@@ -163,6 +163,19 @@ def sd_riemann_solver(u, f, v1, v2, v3, dim, viscous, cfg):
     _call("spdk_sd_riemann_solver", _r(sd(u)), _r(sd(f)), I(v1), I(v2), I(v3), I(dim), I(int(viscous)), _r(cfg))
 
 
+def sd_rusanov_solver(u, f, dim):
+    _call("spdk_sd_rusanov_solver", _r(sd(u)), _r(sd(f)), I(dim))
+
+
+def compute_gradient(u, du, h, dfp_to_sp, dim, cfg):
+    _call("spdk_compute_gradient", _r(sd(u)), _r(sd(du)), D(h), _r(mat(dfp_to_sp)), I(dim), _r(cfg))
+
+
+def compute_viscous_flux(u, du1, v1, du2, v2, du3, v3, sp_to_fp, nu, beta, dim, cfg):
+    _call("spdk_compute_viscous_flux", _r(sd(u)), _r(sd(du1)), I(v1), _r(sd(du2)), I(v2), _r(sd(du3)), I(v3),
+          _r(mat(sp_to_fp)), D(nu), D(beta), I(dim), _r(cfg))
+
+
 def boundaries_sd(u, dim, bc_type):
     _call("spdk_boundaries_sd", _r(sd(u)), I(dim), I(bc_type))
 

@@ -35,6 +35,18 @@ def test_matches_reference_fixture(case):
     g.close()
 
 
+@pytest.mark.parametrize("case", sorted(M.get("viscous_cases", {})))
+def test_viscous_run_matches_reference_fixture(case):
+    """hydro/nu > 0 (interface states, gradients, viscous fluxes, interface
+    sums, diffusion dt limit), 2D/3D, ADER/SSP-RK2, with and without the
+    fallback: the reference's W_cv and step count, bit for bit"""
+    info = M["viscous_cases"][case]
+    w, steps, g = gpu_run(info["overrides"])
+    assert steps == info["steps"]
+    assert same_bits(w, fixture(case)), rel_l1(fixture(case), w)
+    g.close()
+
+
 @pytest.mark.parametrize("case", sorted(M.get("bench_cases", {})))
 def test_benchmark_geometry_matches_reference(case):
     """The benchmark workload itself (2D point blast, NAD+MUSCL, outflow) at
@@ -125,6 +137,15 @@ RANDOM_CASES = {
                        "mesh/x3_bc=reflective"],
     "3d_p3_rk2": ["job/fallback=false", "mesh/nx1=2", "mesh/nx2=3", "mesh/nx3=2", "time/integrator=rk2",
                   "hydro/g3=0.3"],
+    # viscous terms on every boundary kind, ADER and SSP-RK, with the fallback
+    "2d_p3_viscous_fallback_reflective": ["job/fallback=true", "mesh/nx1=6", "mesh/nx2=4", "mesh/nx3=1",
+                                          "mesh/x1_bc=reflective", "mesh/x2_bc=gradfree", "hydro/nu=0.02"],
+    "2d_p2_rk3_viscous_beta": ["job/fallback=false", "mesh/p=2", "mesh/nx1=6", "mesh/nx2=6", "mesh/nx3=1",
+                               "time/integrator=rk3", "hydro/nu=0.05", "hydro/beta=0.01"],
+    "2d_p4_viscous_gravity": ["job/fallback=false", "mesh/p=4", "mesh/nx1=4", "mesh/nx2=6", "mesh/nx3=1",
+                              "hydro/nu=0.01", "hydro/g2=-0.3", "mesh/x2_bc=reflective"],
+    "3d_p2_viscous_fallback": ["job/fallback=true", "mesh/p=2", "mesh/nx1=3", "mesh/nx2=2", "mesh/nx3=3",
+                               "mesh/x3_bc=reflective", "mesh/x1_bc=gradfree", "hydro/nu=0.01"],
 }
 
 

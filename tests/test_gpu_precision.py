@@ -69,6 +69,10 @@ SMOOTH_CASES = {
     "3d_p5_ader": ["job/fallback=false", "mesh/p=5", "mesh/nx1=2", "mesh/nx2=2", "mesh/nx3=2", "time/cfl=0.4"],
     "3d_p2_rk2": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=4",
                   "time/integrator=rk2"],
+    # viscous terms (hydro/nu > 0): the diffusion dt limit is FP64 in both forms
+    "2d_p3_ader_viscous": ["job/fallback=false", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=1", "hydro/nu=0.01"],
+    "3d_p2_rk2_viscous": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=3",
+                          "time/integrator=rk2", "hydro/nu=0.02", "hydro/beta=0.003"],
 }
 
 

@@ -43,6 +43,9 @@ class Mirror:
             if c["integrator"] != "ader" and name == "invader":
                 continue
             self.a[name] = torch.from_numpy(o.array(name).reshape(o.array(name).shape[:2]).copy()).cuda()
+        if c.get("nu", 0.0) > 0:
+            for x in "xyz":
+                self.a["dU" + x + "_sp"] = torch.from_numpy(o.array("dU" + x + "_sp")).cuda()
         self.a["T_sweep"] = torch.zeros_like(self.a["U_sp"])
         self.a["U0_sp"] = torch.zeros_like(self.a["U_sp"])
         self.a["theta_tmp"] = torch.zeros_like(self.a["theta"])
@@ -68,15 +71,30 @@ def xyz(M, prefix):
 
 
 def solve_fluxes(M, P, cfg):
-    """src/hydro_ader.hpp:278-289"""
+    """src/hydro_ader.hpp:278-289, with the viscous terms of :284-288 and
+    :383-405 when hydro/nu > 0"""
+    nu = M.c.get("nu", 0.0)
+    fp = ["U_ader_fp_" + x for x in "xyz"]
     for d in dirs(M):
-        P.transform_a_to_b_1d(M["U_ader_sp"], M["U_ader_fp_" + "xyz"[d]], M["sp_to_fp"], d)
+        P.transform_a_to_b_1d(M["U_ader_sp"], M[fp[d]], M["sp_to_fp"], d)
     for d in dirs(M):
-        P.compute_fluxes(M["U_ader_fp_" + "xyz"[d]], M["F_ader_fp_" + "xyz"[d]], *P.V123[d], cfg)
+        P.compute_fluxes(M[fp[d]], M["F_ader_fp_" + "xyz"[d]], *P.V123[d], cfg)
     for d in dirs(M):
-        P.boundaries_sd(M["U_ader_fp_" + "xyz"[d]], d, BC[M.c["bc"][d]])
+        P.boundaries_sd(M[fp[d]], d, BC[M.c["bc"][d]])
     for d in dirs(M):
-        P.sd_riemann_solver(M["U_ader_fp_" + "xyz"[d]], M["F_ader_fp_" + "xyz"[d]], *P.V123[d], d, 0, cfg)
+        P.sd_riemann_solver(M[fp[d]], M["F_ader_fp_" + "xyz"[d]], *P.V123[d], d, int(nu > 0), cfg)
+    if nu > 0:
+        dU = [M["dU" + x + "_sp"] for x in "xyz"]
+        for d in dirs(M):
+            P.compute_gradient(M[fp[d]], dU[d], h(M)[d], M["dfp_to_sp"], d, cfg)
+        for d in dirs(M):
+            v1, v2, v3 = P.V123[d]
+            P.compute_viscous_flux(M[fp[d]], dU[d], v1, dU[(d + 1) % 3], v2, dU[(d + 2) % 3], v3, M["sp_to_fp"], nu,
+                                   M.c["beta"], d, cfg)
+        for d in dirs(M):
+            P.boundaries_sd(M[fp[d]], d, BC[M.c["bc"][d]])
+        for d in dirs(M):
+            P.sd_rusanov_solver(M[fp[d]], M["F_ader_fp_" + "xyz"[d]], d)
 
 
 def flux_args(M):
@@ -170,7 +188,7 @@ def step(M, P, cfg, dt):
                 P.combine_solution(M["U_sp"], M["U0_sp"], rk_a[st])
     P.compute_primitives(M["U_sp"], M["W_sp"], cfg)
     P.transform_a_to_b(M["W_sp"], M["W_cv"], M["T_sweep"], M["sp_to_cv"], cfg)
-    P.compute_dt(M["W_cv"], dx, dy, dz, 0.0, M.dt_dev, cfg)
+    P.compute_dt(M["W_cv"], dx, dy, dz, c.get("nu", 0.0), M.dt_dev, cfg)
 
 
 CASES = {
@@ -184,6 +202,14 @@ CASES = {
                             "mesh/x3_bc=reflective"],
     "3d_p3_rk2_gravity": ["job/fallback=false", "mesh/nx1=2", "mesh/nx2=3", "mesh/nx3=2", "time/integrator=rk2",
                           "hydro/g3=0.3"],
+    # viscous terms (hydro/nu > 0): interface states, gradients, viscous
+    # fluxes, interface sums and the diffusion dt limit
+    "2d_p3_ader_viscous_fallback": ["job/fallback=true", "mesh/nx1=5", "mesh/nx2=4", "mesh/nx3=1", "hydro/nu=0.02"],
+    "2d_p2_rk3_viscous_reflective": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=5", "mesh/nx3=1",
+                                     "time/integrator=rk3", "mesh/x2_bc=reflective", "mesh/x1_bc=gradfree",
+                                     "hydro/nu=0.05", "hydro/beta=0.01"],
+    "3d_p2_ader_viscous": ["job/fallback=false", "mesh/p=2", "mesh/nx1=3", "mesh/nx2=2", "mesh/nx3=3",
+                           "mesh/x3_bc=reflective", "hydro/nu=0.01"],
 }
 
 
@@ -245,6 +271,26 @@ def test_flux_pass_and_prediction_match_oracle():
                         *h(M), cfg)
     torch.cuda.synchronize()
     assert M.same("U_ader_sp")
+
+
+def test_viscous_flux_pass_matches_oracle():
+    """one flux pass with hydro/nu > 0: after the interface states, the
+    gradients at the solution points, the viscous fluxes (with their ghost
+    fill) and the interface sums, every array equals the oracle's"""
+    import torch
+    import spd_k_b200.proto as P
+    o, c = random_oracle(["job/fallback=false", "mesh/nx1=4", "mesh/nx2=5", "mesh/nx3=1", "hydro/nu=0.03",
+                          "mesh/x1_bc=reflective", "mesh/x2_bc=gradfree"], 11)
+    M = Mirror(o, c)
+    cfg = P.proto_cfg(c)
+    o.call("copy_ader")
+    o.call("solve_fluxes")
+    copy_ader(M)
+    solve_fluxes(M, P, cfg)
+    torch.cuda.synchronize()
+    for name in ("dUx_sp", "dUy_sp", "U_ader_fp_x", "U_ader_fp_y", "F_ader_fp_x", "F_ader_fp_y"):
+        assert M.same(name), name
+    assert float(np.abs(o.array("dUx_sp")).max()) > 0
 
 
 def test_bad_arguments_are_rejected():

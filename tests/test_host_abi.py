@@ -62,6 +62,20 @@ def test_bad_config_is_rejected_without_a_device(lib):
     c = gpu_config(["mesh/nx1=1"])
     rc = lib.spdk_hydro_create(ctypes.byref(make_config(c)), ctypes.byref(h))
     assert rc == -1
+    c = gpu_config(["mesh/nx3=1", "hydro/nu=-0.1"])
+    rc = lib.spdk_hydro_create(ctypes.byref(make_config(c)), ctypes.byref(h))
+    assert rc == -1 and b"nu must be" in lib.spdk_last_error()
+
+
+def test_viscosity_parameters_follow_the_reference_defaults():
+    """hydro/nu opts in, hydro/beta defaults to -2/3 nu (src/main.cpp:236-237)"""
+    from spd_k_b200.api import make_config
+    c = gpu_config(["hydro/nu=0.03"])
+    cfg = make_config(c)
+    assert cfg.nu == 0.03 and cfg.beta == -2. / 3 * 0.03
+    cfg = make_config(gpu_config(["hydro/nu=0.03", "hydro/beta=0.5"]))
+    assert cfg.beta == 0.5
+    assert make_config(gpu_config([])).nu == 0.0
 
 
 @pytest.mark.parametrize("p", range(1, 8))
