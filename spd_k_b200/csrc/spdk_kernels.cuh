@@ -629,8 +629,12 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
         }
     };
     const bool multi = A.in_slices > 1;
+    // a predictor pass whose slices all equal U (the first Picard pass:
+    // copy_ader) has the same flux divergence in every slice: it is
+    // evaluated once and stored for every slice
+    const int nt_eval = (MODE == kPredict && !multi) ? 1 : nt;
     issue(0, 0);
-    for (int t = 0; t < nt; t++) {
+    for (int t = 0; t < nt_eval; t++) {
         // ---- stage slice t (prefetch t+1 into the other buffer) ----
         const int b = multi ? (t & 1) : 0;
         R* Ss = Sbuf + b * NS * SS;
@@ -728,7 +732,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                         if (MODE == kPredict) {
 #pragma unroll
                             for (int tt = 0; tt < NT; tt++)
-                                if (tt == t) dreg[r][v][tt] = dudt;
+                                if (tt == t || (!multi && tt < nt)) dreg[r][v][tt] = dudt;
                         } else {
                             if (G.grav && v != 0) {
                                 const R* uv = Ss + el * SS;
@@ -823,6 +827,14 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
 
     if (MODE == kPredict) {
         // ---- ADER predictor (src/transforms.cpp:309-323) ----
+        __shared__ R Cw[NT * NT];
+        if constexpr (sizeof(R) == 4) {
+            for (int i = tid; i < NT * NT; i += kThreads) {
+                const int tt = i / NT, ll = i % NT;
+                Cw[i] = (tt < nt && ll < nt) ? M.invader[tt * nt + ll] * M.wt[ll] * dt : R(0);
+            }
+            __syncthreads();
+        }
 #pragma unroll
         for (int r = 0; r < PPT; r++) {
             const int q = tid + r * kThreads;
@@ -851,9 +863,17 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
                     for (int tt = 0; tt < NT; tt++) {
                         if (tt >= nt) break;
                         R du = 0;
+                        if constexpr (sizeof(R) == 4) {
+                            // precision form: one product per term with the
+                            // coefficients invader(t,l) w_l dt formed once
 #pragma unroll
-                        for (int ll = 0; ll < NT; ll++)
-                            if (ll < nt) du += dudt[ll] * M.invader[tt * nt + ll] * M.wt[ll] * dt;
+                            for (int ll = 0; ll < NT; ll++)
+                                if (ll < nt) du += dudt[ll] * Cw[tt * NT + ll];
+                        } else {
+#pragma unroll
+                            for (int ll = 0; ll < NT; ll++)
+                                if (ll < nt) du += dudt[ll] * M.invader[tt * nt + ll] * M.wt[ll] * dt;
+                        }
                         const R val = u_old - du;
                         if (v <= D) nw[v][tt] = val;
                         A.ua_out[(((long long)tt * E + ge) * V + v) * NPT + pt] = val;
