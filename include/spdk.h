@@ -84,6 +84,15 @@ typedef struct spdk_hydro_config {
     double nu;             /* kinematic viscosity; > 0 switches the viscous terms on
                               (hydro/nu, src/main.cpp:236; src/hydro.cpp:420-572) */
     double beta;           /* bulk coefficient (hydro/beta, default -2/3 nu, src/main.cpp:237) */
+    /* slab of a domain-decomposed run (0, 0: the whole domain). The solver
+     * holds element rows [slab_lo, slab_lo + N[a]) of a domain of slab_n rows
+     * along its slowest active axis a (y in 2D, z in 3D), which must have a
+     * non-periodic boundary; geometry and initial condition are those rows of
+     * the whole domain's. Halo rows are refreshed by the caller
+     * (spdk_hydro_rows) and the step's dt restricted to the owned rows
+     * (spdk_hydro_slab_dt). No counterpart in the reference (its MPI path is
+     * disabled, src/boundary.cpp:3-24). */
+    int slab_lo, slab_n;
 } spdk_hydro_config;
 
 typedef struct spdk_hydro spdk_hydro;
@@ -152,6 +161,18 @@ int spdk_hydro_profile(spdk_hydro* h, int n, double* ms, long long* launches);
  * SPDK_FIELD_U_SP recomputes W_cv and dt */
 int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count);
 int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count);
+
+/* Domain decomposition (slabs; no counterpart in the reference).
+ * spdk_hydro_rows copies element rows [lo, hi) of U_sp along the slab axis
+ * between the solver and a caller DEVICE buffer of (hi-lo) rows in the
+ * solver's arithmetic (to_solver = 0: solver -> buffer, 1: buffer -> solver),
+ * ordered on the solver stream, asynchronous. spdk_hydro_slab_dt sets the
+ * next dt to the minimum over the element rows [lo, hi) (the owned rows) of
+ * the CFL / diffusion candidates of the current W_cv, on the device; read it
+ * with spdk_hydro_get_dt, reduce across slabs, impose it with
+ * spdk_hydro_set_dt. */
+int spdk_hydro_rows(spdk_hydro* h, int to_solver, int lo, int hi, void* device_buffer);
+int spdk_hydro_slab_dt(spdk_hydro* h, int lo, int hi);
 
 /* Checkpoint / restart (no counterpart in the reference, whose runs start
  * from the initial condition). A checkpoint file holds U_sp in the solver's

@@ -66,6 +66,7 @@ class HydroConfig(ctypes.Structure):
         ("q", ctypes.c_double * 16), ("seed", ctypes.c_ulonglong),
         ("precision", ctypes.c_int), ("device", ctypes.c_int),
         ("nu", ctypes.c_double), ("beta", ctypes.c_double),
+        ("slab_lo", ctypes.c_int), ("slab_n", ctypes.c_int),
     ]
 
 
@@ -129,6 +130,8 @@ def load_library(path=LIB_PATH):
     L.spdk_hydro_restore.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ci]
     ip = ctypes.POINTER(ctypes.c_int)
     L.spdk_checkpoint_peek.argtypes = [ctypes.c_char_p, ci, ip, ip, ip, ip, ip]
+    L.spdk_hydro_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    L.spdk_hydro_slab_dt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
     _lib = L
     return L
 
@@ -253,6 +256,7 @@ def make_config(c, device=0):
     o.device = device
     o.nu = c.get("nu", 0.0)
     o.beta = c.get("beta", -2. / 3 * o.nu)
+    o.slab_lo, o.slab_n = int(c.get("slab_lo", 0)), int(c.get("slab_n", 0))
     return o
 
 
@@ -315,6 +319,21 @@ class HydroSolver:
 
     def step(self):
         _check(_lib.spdk_hydro_step(self.h))
+
+    def rows_to(self, lo, hi, buf):
+        """element rows [lo, hi) of U_sp along the slab axis -> device tensor buf
+        (solver arithmetic), ordered on the solver stream"""
+        _check(_lib.spdk_hydro_rows(self.h, 0, lo, hi, ctypes.c_void_p(buf.data_ptr())))
+
+    def rows_from(self, lo, hi, buf):
+        """device tensor buf -> element rows [lo, hi) of U_sp"""
+        _check(_lib.spdk_hydro_rows(self.h, 1, lo, hi, ctypes.c_void_p(buf.data_ptr())))
+
+    def slab_dt(self, lo, hi):
+        """next dt = minimum of the CFL / diffusion candidates over element rows
+        [lo, hi) of the current W_cv; returns it"""
+        _check(_lib.spdk_hydro_slab_dt(self.h, lo, hi))
+        return self.dt()
 
     def steps(self, n):
         _check(_lib.spdk_hydro_steps(self.h, n))

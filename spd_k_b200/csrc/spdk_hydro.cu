@@ -241,6 +241,27 @@ int enqueue_step(spdk_hydro* h) {
     return rc;
 }
 
+// dt candidates of the W_cv points of elements [e_lo, e_hi) (a slab's owned
+// rows), the same per-point formula as the step's epilogues
+template <typename R, int D>
+__global__ void __launch_bounds__(kThreads) slab_dt_kernel(DevGrid G, const R* __restrict__ wcv, long long e_lo,
+                                                          long long e_hi, int n, int NPT,
+                                                          unsigned long long* dtmin) {
+    constexpr int V = D + 2;
+    double dtl = 1.7976931348623157e308;
+    const long long cnt = (e_hi - e_lo) * NPT;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long e = e_lo + q / NPT;
+        const int pt = (int)(q % NPT);
+        R w[V];
+#pragma unroll
+        for (int v = 0; v < V; v++) w[v] = wcv[(e * V + v) * NPT + pt];
+        dtl = smin(dtl, point_dt<D>(G, w, n));
+    }
+    block_min_dt(dtl, dtmin);
+}
+
 __global__ void narrow_kernel(const double* __restrict__ a, float* __restrict__ b, long long n) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
@@ -305,6 +326,13 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         return fail(SPDK_E_ARG, "rk_order must be 1, 2 or 3");
     if (!(c.nu >= 0.0) || !std::isfinite(c.nu) || !std::isfinite(c.beta))
         return fail(SPDK_E_ARG, "nu must be >= 0 and nu, beta finite");
+    if (c.slab_n != 0 || c.slab_lo != 0) {
+        const int rows = c.N[D - 1];
+        if (c.slab_lo < 0 || c.slab_n < rows || c.slab_lo + rows > c.slab_n)
+            return fail(SPDK_E_ARG, "slab rows [slab_lo, slab_lo + N) must lie inside the slab_n rows of the domain");
+        if (c.bc[D - 1] == SPDK_BC_PERIODIC)
+            return fail(SPDK_E_ARG, "the slab axis (y in 2D, z in 3D) needs a non-periodic boundary");
+    }
 
     spdk_hydro* h = new spdk_hydro();
     h->cfg = c;
@@ -335,7 +363,10 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     int rc = cudaSetDevice(c.device) == cudaSuccess ? 0 : fail(SPDK_E_CUDA, "cudaSetDevice failed");
     if (rc) { delete h; return rc; }
     build_matrices(c.p, ader, &h->mats);
-    for (int d = 0; d < 3; d++) build_axis(N[d], c.p, c.L[d], h->mats.x_fp, d < D, &h->ax[d]);
+    for (int d = 0; d < 3; d++) {
+        const bool slab = d == D - 1 && c.slab_n > 0;
+        build_axis(N[d], c.p, c.L[d], h->mats.x_fp, d < D, &h->ax[d], slab ? c.slab_lo : 0, slab ? c.slab_n : 0);
+    }
     // device matrices (same values as the host setup)
     const int n = h->n, nf = h->nf;
     std::memset(&h->dm64, 0, sizeof(h->dm64));
@@ -685,6 +716,45 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
     SPDK_CUDA(cudaGetLastError());
     SPDK_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int spdk_hydro_rows(spdk_hydro* h, int to_solver, int lo, int hi, void* device_buffer) {
+    if (!h || !device_buffer) return fail(SPDK_E_ARG, "null argument");
+    const int nrows = h->G.N[h->D - 1];
+    if (lo < 0 || hi > nrows || lo >= hi) return fail(SPDK_E_ARG, "rows out of range");
+    const size_t row = (size_t)(h->E / nrows) * h->V * h->NPT * h->esz;
+    char* u = (char*)h->u + (size_t)lo * row;
+    const size_t bytes = (size_t)(hi - lo) * row;
+    if (to_solver) {
+        SPDK_CUDA(cudaMemcpyAsync(u, device_buffer, bytes, cudaMemcpyDeviceToDevice, h->stream));
+        h->feat_valid = false;
+    } else {
+        SPDK_CUDA(cudaMemcpyAsync(device_buffer, u, bytes, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    return 0;
+}
+
+int spdk_hydro_slab_dt(spdk_hydro* h, int lo, int hi) {
+    if (!h) return fail(SPDK_E_ARG, "null argument");
+    const int nrows = h->G.N[h->D - 1];
+    if (lo < 0 || hi > nrows || lo >= hi) return fail(SPDK_E_ARG, "rows out of range");
+    const long long per = h->E / nrows;
+    const long long cnt = (long long)(hi - lo) * per * h->NPT;
+    long long blocks = (cnt + kThreads - 1) / kThreads;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
+    SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
+    const long long e_lo = lo * per, e_hi = hi * per;
+    if (h->prec == SPDK_PRECISION_FP32) {
+        if (h->D == 2) slab_dt_kernel<float, 2><<<(unsigned)blocks, kThreads, 0, h->stream>>>(h->G, (const float*)h->wcv, e_lo, e_hi, h->n, h->NPT, h->dtmin);
+        else slab_dt_kernel<float, 3><<<(unsigned)blocks, kThreads, 0, h->stream>>>(h->G, (const float*)h->wcv, e_lo, e_hi, h->n, h->NPT, h->dtmin);
+    } else {
+        if (h->D == 2) slab_dt_kernel<double, 2><<<(unsigned)blocks, kThreads, 0, h->stream>>>(h->G, (const double*)h->wcv, e_lo, e_hi, h->n, h->NPT, h->dtmin);
+        else slab_dt_kernel<double, 3><<<(unsigned)blocks, kThreads, 0, h->stream>>>(h->G, (const double*)h->wcv, e_lo, e_hi, h->n, h->NPT, h->dtmin);
+    }
+    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
+    SPDK_CUDA(cudaGetLastError());
     return 0;
 }
 

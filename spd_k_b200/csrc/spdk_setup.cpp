@@ -315,11 +315,11 @@ void build_matrices(int p, bool ader, Matrices* m) {
     }
 }
 
-void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a) {
+void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a, int lo, int N_all) {
     *a = Axis{};
     a->N = N;
     a->active = active;
-    a->h = L / N;
+    a->h = L / (N_all > 0 ? N_all : N);
     if (!active) return;
     const int nsp = p + 1, nfp = p + 2, Ntot = N + 2;
     a->n = nsp;
@@ -332,7 +332,7 @@ void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a
     a->fv_centers.assign(a->fvn, 0.0);
     for (int j = 0; j < Ntot; j++) {
         for (int i = 0; i < nfp; i++) {
-            const double f = (0 + j - 1 + x_fp[i]) * a->h;
+            const double f = (lo + j - 1 + x_fp[i]) * a->h;
             a->sd_faces[j * nfp + i] = f;
             const int g = i + j * nsp;
             if (g >= idL && g < idR) a->fv_faces[i - idL + j * nsp] = f;

@@ -43,7 +43,9 @@ struct Axis {
     std::vector<double> fv_faces;    // fvn + 1
     std::vector<double> fv_centers;  // fvn
 };
-void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a);
+// N elements of an axis of N_all elements over length L, starting at element
+// `lo` of it (a slab; lo = 0, N_all = N for the whole axis)
+void build_axis(int N, int p, double L, const double* x_fp, bool active, Axis* a, int lo = 0, int N_all = 0);
 
 // Initial state: W_cv (primitive sub-cell averages) of the active elements
 // in the solver layout [element][var][point], V = D+2 slots, evaluated by
