@@ -3,8 +3,11 @@
 // rounds exactly as the reference's CPU build does.
 #include "spdk_setup.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 namespace spdk {
 
@@ -354,46 +357,66 @@ void initial_wcv(const spdk_hydro_config& c, const Matrices& m, const Axis ax[3]
     const int Nx = ax[0].N, Ny = ax[1].N, Nz = D == 3 ? ax[2].N : 1;
     const bool ay = true, az = D == 3;
     wcv->assign((size_t)Nx * Ny * Nz * V * npt, 0.0);
+    // every element is independent (a pure function of its positions), so
+    // the elements are split across host threads; the values do not depend
+    // on the split
+    const long long E = (long long)Nx * Ny * Nz;
+    const long long work = E * npt * (long long)npt;  // point evaluations per variable
+    unsigned nth = std::max(1u, std::thread::hardware_concurrency());
+    if (work < (1LL << 22)) nth = 1;
+    nth = (unsigned)std::min<long long>(nth, std::max<long long>(1, E));
     // slot of primitive var in the solver layout (rho, v_1..v_D, p)
-    for (int k = 0; k < Nz; k++)
-        for (int j = 0; j < Ny; j++)
-            for (int i = 0; i < Nx; i++) {
-                const size_t e = ((size_t)k * Ny + j) * Nx + i;
-                // ghost-inclusive element indices of the reference geometry
-                const int gi = i + 1, gj = j + 1, gk = az ? k + 1 : 0;
-                const double* fx = &ax[0].sd_faces[(size_t)gi * nf];
-                const double* fy = &ax[1].sd_faces[(size_t)gj * nf];
-                const double* fz = az ? &ax[2].sd_faces[(size_t)gk * nf] : nullptr;
-                const int pz = az ? n : 1;
-                for (int kk = 0; kk < pz; kk++)
-                    for (int jj = 0; jj < n; jj++)
-                        for (int ii = 0; ii < n; ii++) {
-                            const int pt = (kk * n + jj) * n + ii;
-                            for (int var = 0; var < 5; var++) {
-                                int slot;
-                                if (var == 0) slot = 0;
-                                else if (var == 4) slot = D + 1;
-                                else if (var <= D) slot = var;
-                                else continue;  // z velocity of a 2D run: identically zero
-                                double value = 0, x, y = 0, z = 0;
-                                for (int nn = 0; nn < pz; nn++) {
-                                    if (az) z = fz[kk] + m.xx[nn] * (fz[kk + 1] - fz[kk]);
-                                    for (int mm = 0; mm < n; mm++) {
-                                        if (ay) y = fy[jj] + m.xx[mm] * (fy[jj + 1] - fy[jj]);
-                                        for (int ll = 0; ll < n; ll++) {
-                                            x = fx[ii] + m.xx[ll] * (fx[ii + 1] - fx[ii]);
-                                            double s = ic_point(c, var, x, y, z, ay, az);
-                                            s *= m.wx[ll];
-                                            if (ay) s *= m.wx[mm];
-                                            if (az) s *= m.wx[nn];
-                                            value += s;
-                                        }
+    auto body = [&](long long e_begin, long long e_end) {
+        for (long long e_it = e_begin; e_it < e_end; e_it++) {
+            const int i = (int)(e_it % Nx), j = (int)((e_it / Nx) % Ny), k = (int)(e_it / ((long long)Nx * Ny));
+            const size_t e = (size_t)e_it;
+            // ghost-inclusive element indices of the reference geometry
+            const int gi = i + 1, gj = j + 1, gk = az ? k + 1 : 0;
+            const double* fx = &ax[0].sd_faces[(size_t)gi * nf];
+            const double* fy = &ax[1].sd_faces[(size_t)gj * nf];
+            const double* fz = az ? &ax[2].sd_faces[(size_t)gk * nf] : nullptr;
+            const int pz = az ? n : 1;
+            for (int kk = 0; kk < pz; kk++)
+                for (int jj = 0; jj < n; jj++)
+                    for (int ii = 0; ii < n; ii++) {
+                        const int pt = (kk * n + jj) * n + ii;
+                        for (int var = 0; var < 5; var++) {
+                            int slot;
+                            if (var == 0) slot = 0;
+                            else if (var == 4) slot = D + 1;
+                            else if (var <= D) slot = var;
+                            else continue;  // z velocity of a 2D run: identically zero
+                            double value = 0, x, y = 0, z = 0;
+                            for (int nn = 0; nn < pz; nn++) {
+                                if (az) z = fz[kk] + m.xx[nn] * (fz[kk + 1] - fz[kk]);
+                                for (int mm = 0; mm < n; mm++) {
+                                    if (ay) y = fy[jj] + m.xx[mm] * (fy[jj + 1] - fy[jj]);
+                                    for (int ll = 0; ll < n; ll++) {
+                                        x = fx[ii] + m.xx[ll] * (fx[ii + 1] - fx[ii]);
+                                        double s = ic_point(c, var, x, y, z, ay, az);
+                                        s *= m.wx[ll];
+                                        if (ay) s *= m.wx[mm];
+                                        if (az) s *= m.wx[nn];
+                                        value += s;
                                     }
                                 }
-                                (*wcv)[(e * V + slot) * npt + pt] = value;
                             }
+                            (*wcv)[(e * V + slot) * npt + pt] = value;
                         }
-            }
+                    }
+        }
+    };
+    if (nth == 1) {
+        body(0, E);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const long long chunk = (E + nth - 1) / nth;
+    for (unsigned t = 0; t < nth; t++) {
+        const long long b = (long long)t * chunk, en = std::min(E, b + chunk);
+        if (b < en) pool.emplace_back(body, b, en);
+    }
+    for (std::thread& th : pool) th.join();
 }
 
 }  // namespace spdk

@@ -112,6 +112,9 @@ IC_CASES = [
     ["mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=1", "problem/problem=user"],
     ["mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=2", "problem/problem=kh_noise", "mesh/p=5"],
     ["mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=1", "problem/problem=rti_top", "hydro/g2=-0.1"],
+    # large enough (>= 2^22 point evaluations) for the host-threaded quadrature
+    ["mesh/nx1=128", "mesh/nx2=136", "mesh/nx3=1", "problem/problem=rti_top", "hydro/g2=-0.1"],
+    ["mesh/nx1=6", "mesh/nx2=6", "mesh/nx3=6", "problem/problem=kh_noise", "mesh/p=5"],
 ]
 
 
