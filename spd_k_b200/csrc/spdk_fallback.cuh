@@ -387,15 +387,19 @@ struct ThetaTile {
 };
 
 // called by every thread of the block; `scratch` holds ThetaTile::scratch
-// bytes; th (tile + 1 halo) is complete after the caller's next barrier
+// bytes; th (tile + 1 halo) is complete after the caller's next barrier.
+// Returns (to every thread) whether any trouble lies within reach of the
+// tile: when none does, theta is zero on the tile + 1 halo and the blending
+// passes are skipped.
 template <int D, int P, int TX, int TY, int TZ>
-__device__ __forceinline__ void theta_on_tile(const DevGrid& G, const uint8_t* __restrict__ T, const int o[3],
-                                              uint8_t* scratch, uint8_t* th, uint8_t* __restrict__ theta_out) {
+__device__ __forceinline__ int theta_on_tile(const DevGrid& G, const uint8_t* __restrict__ T, const int o[3],
+                                             uint8_t* scratch, uint8_t* th, uint8_t* __restrict__ theta_out) {
     using TT = ThetaTile<D, P, TX, TY, TZ>;
     constexpr int n = P + 1;
     const int dz = D == 3 ? 1 : 0;
     uint8_t* T3 = scratch;
     uint8_t* Th2 = scratch + TT::n3;
+    int any = 0;
     for (int q = threadIdx.x; q < TT::n3; q += blockDim.x) {
         int a[3] = {o[0] - 3 + q % TT::E3x, o[1] - 3 + (q / TT::E3x) % TT::E3y, o[2] - 3 * dz + q / (TT::E3x * TT::E3y)};
         // a cell three layers outside a non-periodic boundary has no image
@@ -406,9 +410,24 @@ __device__ __forceinline__ void theta_on_tile(const DevGrid& G, const uint8_t* _
         for (int d = 0; d < D; d++)
             outside |= G.bc[d] != kPeriodic && (a[d] < -2 || a[d] >= G.N[d] * n + 2);
         bool fl[3];
-        T3[q] = outside ? (uint8_t)0 : T[cell_image<D, P>(G, a, fl)];
+        const uint8_t tq = outside ? (uint8_t)0 : T[cell_image<D, P>(G, a, fl)];
+        T3[q] = tq;
+        any |= tq;
     }
-    __syncthreads();
+    if (!__syncthreads_or(any)) {
+        // no trouble within three cells of the tile: theta is zero on it
+        for (int q = threadIdx.x; q < TT::n1; q += blockDim.x) {
+            th[q] = 0;
+            const int l0[3] = {q % TT::E1x, (q / TT::E1x) % TT::E1y, q / (TT::E1x * TT::E1y)};
+            const bool inner = l0[0] >= 1 && l0[0] <= TT::Bx && l0[1] >= 1 && l0[1] <= TT::By &&
+                               (D == 2 || (l0[2] >= 1 && l0[2] <= TT::Bz));
+            if (inner) {
+                int ga[3] = {o[0] + l0[0] - 1, o[1] + l0[1] - 1, o[2] + l0[2] - dz};
+                theta_out[cell_id<D, P>(G, ga)] = 0;
+            }
+        }
+        return 0;
+    }
     if (G.blending) {
         for (int q = threadIdx.x; q < TT::n2; q += blockDim.x) {
             const int x = q % TT::E2x + 1, y = (q / TT::E2x) % TT::E2y + 1, z = q / (TT::E2x * TT::E2y) + dz;
@@ -460,6 +479,7 @@ __device__ __forceinline__ void theta_on_tile(const DevGrid& G, const uint8_t* _
             theta_out[cell_id<D, P>(G, ga)] = (uint8_t)t8;
         }
     }
+    return 1;
 }
 
 // MUSCL-Hancock face states of cell X for a face of direction Dn
@@ -569,7 +589,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
     const long long E = G.E;
     // theta on the tile + 1 halo from the troubles (scratch: the W_old area,
     // written only after the barrier that follows)
-    theta_on_tile<D, P, TX, TY, TZ>(G, A.trouble, o, reinterpret_cast<uint8_t*>(Wo), th, A.theta);
+    const int near = theta_on_tile<D, P, TX, TY, TZ>(G, A.trouble, o, reinterpret_cast<uint8_t*>(Wo), th, A.theta);
     // SD face fluxes of the tile
     const int nfaces[3] = {SM::NF0, SM::NF1, SM::NF2};
     int fbase[3] = {0, SM::NF0, SM::NF0 + SM::NF1};
@@ -595,11 +615,11 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
         }
     }
     __syncthreads();
-    // faces that blend in the fallback flux
+    // faces that blend in the fallback flux (none when no trouble is near)
     int need = 0;
 #pragma unroll
     for (int d = 0; d < D; d++) {
-        if (need) break;
+        if (need || !near) break;
         const int ex = Bx + (d == 0), ey = By + (d == 1);
         for (int q = threadIdx.x; q < nfaces[d]; q += blockDim.x) {
             int a[3] = {q % ex, (q / ex) % ey, q / (ex * ey)};
@@ -608,7 +628,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
             if (th[sR] | th[sL]) { need = 1; break; }
         }
     }
-    need = __syncthreads_or(need);
+    need = near ? __syncthreads_or(need) : 0;
     if (need) {
         // W_old = prim(U_cv) on the tile + 2 halo, reflective images flipped
         for (int q = threadIdx.x; q < E2x * E2y * SM::E2z; q += blockDim.x) {
