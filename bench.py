@@ -459,23 +459,45 @@ def main():
     rc = L.spdk_hydro_get_stream(solver2.h, ctypes.byref(sp))
     stream2 = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
     e2e_steps = max(1, min(args.steps, 200))
+    # simulated time the job runs to: the sum of the dts of e2e_steps steps
+    # from the written state (untimed; the timed run repeats the same dts)
+    solver2.write_u(u_host)
+    t_end = 0.0
+    dt = solver2.dt()
+    for _ in range(e2e_steps):
+        solver2.step()
+        t_end += dt
+        dt = solver2.dt()
     barrier(dist)
     solver2.sync()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream2)
-    solver2.write_u(u_host)                 # H2D of the job's input state (pinned)
-    for _ in range(e2e_steps):
-        solver2.step()                      # spdk_hydro_step
-        solver2.dt()                        # blocking D2H of the step's dt, as time_evolution does
-    solver2.read(S.FIELD_W_CV, out=w_host)  # D2H of the result
-    f1.record(stream2)
-    f1.synchronize()
-    e2e_ms = max_over_ranks(dist, f0.elapsed_time(f1), f"cuda:{local}")
+
+    def timed(run):
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream2)
+        solver2.write_u(u_host)                 # H2D of the job's input state (pinned)
+        n = run()
+        solver2.read(S.FIELD_W_CV, out=w_host)  # D2H of the result
+        f1.record(stream2)
+        f1.synchronize()
+        return n, max_over_ranks(dist, f0.elapsed_time(f1), f"cuda:{local}")
+
+    def per_step():
+        for _ in range(e2e_steps):
+            solver2.step()                      # spdk_hydro_step
+            solver2.dt()                        # blocking D2H of the step's dt (the reference's loop)
+        return e2e_steps
+
+    # time_evolution through the C ABI (spdk_hydro_evolve: the loop on the device)
+    n_evolve, e2e_ms = timed(lambda: solver2.evolve(t_end))
+    n_loop, loop_ms = timed(per_step)
     state_bytes = u_host.nbytes
-    e2e = {"value": world * dof * e2e_steps / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
-           "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": 8 + state_bytes / e2e_steps,
-           "steps": e2e_steps, "path": "spdk_hydro_write + spdk_hydro_step/get_dt per step + spdk_hydro_read"}
+    e2e = {"value": world * dof * n_evolve / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
+           "h2d_bytes_per_step": state_bytes / n_evolve, "d2h_bytes_per_step": state_bytes / n_evolve,
+           "steps": n_evolve, "t_end": t_end,
+           "path": "spdk_hydro_write + spdk_hydro_evolve(t_end) + spdk_hydro_read",
+           "host_step_loop": {"value": world * dof * n_loop / (loop_ms * 1e-3),
+                              "path": "spdk_hydro_step + blocking spdk_hydro_get_dt per step"}}
     solver2.close()
 
     # ---- the other forms on the same workload, beside the timed one ----

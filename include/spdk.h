@@ -137,7 +137,12 @@ int spdk_hydro_step(spdk_hydro* h);
  * graph; asynchronous */
 int spdk_hydro_steps(spdk_hydro* h, int n);
 /* time_evolution: steps until t >= t_end; dt_output > 0 clamps dt to hit
- * output times exactly. Returns the number of steps and the final t. */
+ * output times exactly. Returns the number of steps and the final t. The
+ * loop runs on the device: each step's last kernel advances t, clamps the
+ * next dt and closes a stop gate at t_end (the host loop's FP64 operations,
+ * so the steps and states equal a host loop's bit for bit); the host
+ * launches captured steps in batches and reads the loop state once per
+ * batch. Steps launched past the gate do nothing. */
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t);
 int spdk_hydro_sync(spdk_hydro* h);
 /* the CUDA stream (cudaStream_t) every solver launch is ordered on */

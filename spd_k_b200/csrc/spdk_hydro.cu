@@ -2,6 +2,7 @@
 // declared in include/spdk.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -199,7 +200,8 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
         }
     }
     prof_begin(h);
-    advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
+    if (h->evolve_mode) evolve_advance_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap, h->tb, h->gate);
+    else advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
     prof_end(h, SPDK_KERNEL_OTHER);
     launches++;
     h->launches = launches;
@@ -220,7 +222,11 @@ int refresh_features(spdk_hydro* h) {
 }
 
 int enqueue_step(spdk_hydro* h) {
-    if (h->elem_trouble) SPDK_CUDA(cudaMemsetAsync(h->elem_trouble, 0, (size_t)h->E, h->stream));
+    if (h->elem_trouble) {
+        clear_labels_kernel<<<(unsigned)std::min<long long>((h->E + 255) / 256, 1024), 256, 0, h->stream>>>(
+            h->G, h->elem_trouble, h->E);
+        SPDK_CUDA(cudaGetLastError());
+    }
     if (h->mlp) {
         if (int rc = refresh_features(h)) return rc;
         // a-priori flags of the state at the start of the step, on the side
@@ -230,7 +236,7 @@ int enqueue_step(spdk_hydro* h) {
         SPDK_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
         const int N[3] = {h->G.N[0], h->G.N[1], h->G.N[2]};
         const int rc = indicator_flags(h->mlp, h->feat, h->means, h->D, h->p, N, h->G.bc, h->E, h->elem_pred, h->thr,
-                                       h->side);
+                                       h->side, h->G.gate);
         if (rc) return rc;
         SPDK_CUDA(cudaEventRecord(h->ev_join, h->side));
         h->join_pending = true;
@@ -262,6 +268,18 @@ __global__ void __launch_bounds__(kThreads) slab_dt_kernel(DevGrid G, const R* _
     block_min_dt(dtl, dtmin);
 }
 
+__global__ void widen_kernel(const float* __restrict__ a, double* __restrict__ b, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
+// the precision form's host exchange buffer: doubles, converted on the
+// device (allocated on the first read or write of a state field)
+int ensure_stage(spdk_hydro* h) {
+    if (h->stage) return 0;
+    return dalloc(h, &h->stage, (size_t)h->E * h->V * h->NPT * sizeof(double));
+}
+
 __global__ void narrow_kernel(const double* __restrict__ a, float* __restrict__ b, long long n) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         b[i] = (float)a[i];
@@ -288,11 +306,12 @@ int set_attributes(const KernelSetT<R>& ks) {
 void release(spdk_hydro* h) {
     checkpoint_release(h);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph_evolve) cudaGraphExecDestroy(h->graph_evolve);
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     void* ptrs[] = {h->u, h->ua[0], h->ua[1], h->u0, h->ucv[0], h->ucv[1], h->ff[0], h->ff[1], h->ff[2],
                     h->wcv, h->dt, h->fvf[0], h->fvf[1], h->fvf[2], h->fvc[0], h->fvc[1], h->fvc[2],
                     h->rpo, h->rpn, h->trouble, h->theta, h->dtmin, h->status, h->elem_trouble, h->elem_pred,
-                    h->feat, h->means, h->vg[0], h->vg[1], h->vg[2]};
+                    h->feat, h->means, h->vg[0], h->vg[1], h->vg[2], h->gate, h->tb, h->stage};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
@@ -439,6 +458,9 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
     if (!rc) rc = dalloc(h, (void**)&h->dt, sizeof(double) * 2);
     if (!rc) rc = dalloc(h, (void**)&h->dtmin, sizeof(unsigned long long));
     if (!rc) rc = dalloc(h, (void**)&h->status, sizeof(int));
+    if (!rc) rc = dalloc(h, (void**)&h->gate, sizeof(int));
+    if (!rc) rc = dalloc(h, (void**)&h->tb, 8 * sizeof(double));
+    if (!rc && cudaMemset(h->gate, 0, sizeof(int)) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset gate");
     if (!rc && cudaMemset(h->status, 0, sizeof(int)) != cudaSuccess) rc = fail(SPDK_E_CUDA, "memset status");
     G.status = h->status;
     if (!rc && c.fallback) {
@@ -534,7 +556,7 @@ int spdk_hydro_get_info(const spdk_hydro* h, spdk_hydro_info* info) {
     int l = 0;
     for (int s = 0; s < h->nstages; s++) l += (h->nt - 1) + (h->cfg.fallback ? 1 + 2 * h->nt : 1);
     if (h->vg[0]) l += h->nstages * h->nt;  // a viscous pre-pass before every Picard pass
-    info->launches_per_step = l + 1 + (h->mlp ? 2 : 0);
+    info->launches_per_step = l + 1 + (h->mlp ? 2 : 0) + (h->elem_trouble ? 1 : 0);
     info->device_bytes = h->bytes;
     return 0;
 }
@@ -618,31 +640,48 @@ int spdk_hydro_sync(spdk_hydro* h) {
 
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t_out) {
     if (!h) return fail(SPDK_E_ARG, "null argument");
-    // src/hydro_ader.hpp:215-273 with a blocking dt read per step, as there
-    double t = 0, dt = 0;
-    long long ns = 0;
-    int rc = spdk_hydro_get_dt(h, &dt);
-    if (rc) return rc;
-    const bool outputs = dt_output > 0;
-    double t_output = dt_output;
-    while (t < t_end) {
-        rc = enqueue_step(h);
+    // src/hydro_ader.hpp:215-273 as a device-resident loop: the step's dt,
+    // t, the output clamping and the stop test live on the device
+    // (evolve_advance_kernel, the host loop's operations), so the host
+    // launches captured steps in batches and reads the loop state once per
+    // batch instead of once per step. Steps launched after t reaches t_end
+    // find the gate closed and do nothing.
+    if (steps) *steps = 0;
+    if (t_out) *t_out = 0;
+    if (!(0.0 < t_end)) return 0;
+    if (int rc = refresh_features(h)) return rc;
+    if (!h->graph_evolve) {
+        cudaGraph_t g;
+        DevGrid keep = h->G;
+        h->G.gate = h->gate;
+        h->evolve_mode = true;
+        SPDK_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        h->evolve_mode = false;
+        h->G = keep;
         if (rc) return rc;
-        t += dt;
-        ns++;
-        rc = spdk_hydro_get_dt(h, &dt);
-        if (rc) return rc;
-        if (outputs) {
-            if (t >= t_output) t_output = t + dt_output;
-            if (t + dt > t_output) {
-                dt = t_output - t;
-                rc = spdk_hydro_set_dt(h, dt);
-                if (rc) return rc;
-            }
-        }
+        if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&h->graph_evolve, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
     }
-    if (steps) *steps = ns;
-    if (t_out) *t_out = t;
+    const double tb0[5] = {0.0, dt_output, 0.0, t_end, dt_output > 0 ? dt_output : -1.0};
+    SPDK_CUDA(cudaMemcpyAsync(h->tb, tb0, sizeof(tb0), cudaMemcpyHostToDevice, h->stream));
+    SPDK_CUDA(cudaMemsetAsync(h->gate, 0, sizeof(int), h->stream));
+    double st[3] = {0, 0, 0};
+    int closed = 0;
+    for (int batch = 8; !closed; batch = std::min(batch * 2, 64)) {
+        for (int q = 0; q < batch; q++) SPDK_CUDA(cudaGraphLaunch(h->graph_evolve, h->stream));
+        SPDK_CUDA(cudaMemcpyAsync(st, h->tb, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaMemcpyAsync(&closed, h->gate, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaStreamSynchronize(h->stream));
+        if (int rc = check_status(h)) return rc;
+    }
+    // the stream now only holds no-op launches; reopen the gate for later steps
+    SPDK_CUDA(cudaMemsetAsync(h->gate, 0, sizeof(int), h->stream));
+    if (steps) *steps = (long long)st[2];
+    if (t_out) *t_out = st[0];
     return 0;
 }
 
@@ -654,11 +693,12 @@ int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count) {
         if (count != state) return fail(SPDK_E_ARG, "count must be E*V*NPT = " + std::to_string(state));
         const void* src = field == SPDK_FIELD_U_SP ? h->u : h->wcv;
         if (h->prec == SPDK_PRECISION_FP32) {
-            // FP32 values widened exactly to doubles
-            std::vector<float> b(state);
-            SPDK_CUDA(cudaMemcpyAsync(b.data(), src, state * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+            // FP32 values widened exactly to doubles on the device
+            if (int rc = ensure_stage(h)) return rc;
+            widen_kernel<<<1024, 256, 0, h->stream>>>((const float*)src, (double*)h->stage, (long long)state);
+            SPDK_CUDA(cudaGetLastError());
+            SPDK_CUDA(cudaMemcpyAsync(host, h->stage, state * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
             SPDK_CUDA(cudaStreamSynchronize(h->stream));
-            for (size_t q = 0; q < state; q++) host[q] = b[q];
             return 0;
         }
         SPDK_CUDA(cudaMemcpyAsync(host, src, state * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -697,15 +737,16 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
     const unsigned long long maxbits = 0x7FEFFFFFFFFFFFFFULL;
     h->feat_valid = false;
     if (h->prec == SPDK_PRECISION_FP32) {
-        // doubles rounded once to FP32
-        std::vector<float> b(host, host + state);
-        SPDK_CUDA(cudaMemcpyAsync(h->u, b.data(), state * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+        // doubles rounded once to FP32, on the device
+        if (int rc = ensure_stage(h)) return rc;
+        SPDK_CUDA(cudaMemcpyAsync(h->stage, host, state * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        narrow_kernel<<<1024, 256, 0, h->stream>>>((const double*)h->stage, (float*)h->u, (long long)state);
         SPDK_CUDA(cudaMemcpyAsync(h->dtmin, &maxbits, sizeof(maxbits), cudaMemcpyHostToDevice, h->stream));
         h->ks32.derive<<<(unsigned)h->E, kThreads, 0, h->stream>>>(h->G, h->dm32, (const float*)h->u,
                                                                     (float*)h->wcv, h->dtmin);
         advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
         SPDK_CUDA(cudaGetLastError());
-        // the pageable staging vector must outlive the copy
+        // the caller's buffer must outlive the copy
         SPDK_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     }
@@ -802,10 +843,14 @@ int spdk_hydro_set_indicator(spdk_hydro* h, spdk_mlp* m, float threshold) {
     h->thr = threshold;
     h->feat_valid = false;
     h->G.elem_pred = m ? h->elem_pred : nullptr;
-    // the captured step holds the old kernel arguments
+    // the captured steps hold the old kernel arguments
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;
+    }
+    if (h->graph_evolve) {
+        cudaGraphExecDestroy(h->graph_evolve);
+        h->graph_evolve = nullptr;
     }
     return 0;
 }

@@ -62,6 +62,14 @@ struct spdk_hydro {
     size_t bytes = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    // device-resident time loop (spdk_hydro_evolve): a step graph whose
+    // kernels return once `gate` is set, ending in evolve_advance_kernel on
+    // tb = {t, t_output, steps, t_end, dt_output}
+    cudaGraphExec_t graph_evolve = nullptr;
+    bool evolve_mode = false;  // enqueue_step records the device loop's step end
+    int* gate = nullptr;
+    double* tb = nullptr;
+    void* stage = nullptr;  // precision form: doubles exchanged with the host
     int launches = 0;
     // per-launch event timing (spdk_hydro_profile)
     bool profiling = false;

@@ -62,7 +62,13 @@ struct DevGrid {
     // a-priori prediction that counts all its sub-cells troubled (NULL: off)
     uint8_t* elem_trouble;
     const uint8_t* elem_pred;
+    // device-resident time loop (spdk_hydro_evolve): set once t reaches
+    // t_end; every kernel of a step launched after that returns at once
+    // (NULL: never)
+    const int* gate;
 };
+
+__device__ __forceinline__ bool gate_closed(const DevGrid& G) { return G.gate && *G.gate; }
 
 enum { kPredict = 0, kCorrect = 1, kFlux = 2 };
 
@@ -978,6 +984,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
 // the inviscid kernels carry none of that code
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
 __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+    if (gate_closed(G)) return;
     picard_kernel_body<R, D, P, TX, TY, TZ, MODE, VISC>(G, M, A, blockIdx.x);
 }
 

@@ -92,6 +92,38 @@ static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin, 
     *dtmin = 0x7FEFFFFFFFFFFFFFULL;
 }
 
+// The device-resident time loop's step end (src/hydro_ader.hpp:234-261):
+// t += dt of the step, next dt from the reduction (viscous cap as above),
+// dt clamped to the next output time, and the gate closed once t >= t_end.
+// tb = {t, t_output, steps, t_end, dt_output (<= 0: no outputs)}; the same
+// FP64 operations as the host loop, so the dt sequence is identical.
+static __global__ void evolve_advance_kernel(double* dt, unsigned long long* dtmin, double cap, double* tb,
+                                             int* gate) {
+    if (*gate) return;
+    const double used = *dt;
+    const double v = __longlong_as_double((long long)*dtmin);
+    double next = (cap > 0.0 && !(v < cap)) ? cap : v;
+    *dtmin = 0x7FEFFFFFFFFFFFFFULL;
+    const double t = tb[0] + used;
+    double t_output = tb[1];
+    if (tb[4] > 0) {
+        if (t >= t_output) t_output = t + tb[4];
+        if (t + next > t_output) next = t_output - t;
+    }
+    *dt = next;
+    tb[0] = t;
+    tb[1] = t_output;
+    tb[2] += 1.0;
+    if (!(t < tb[3])) *gate = 1;
+}
+
+// per-element trouble labels of a step <- 0 (skipped once the gate is closed)
+static __global__ void clear_labels_kernel(DevGrid G, uint8_t* labels, long long n) {
+    if (gate_closed(G)) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        labels[i] = 0;
+}
+
 // ---------------------------------------------------------------------------
 // kernel table of one (R, D, P, tile) instantiation
 // ---------------------------------------------------------------------------

@@ -21,7 +21,8 @@ int feature_rows(const void* u, bool fp32, int D, int p, const int N[3], const i
 // part (columns < 2 NPT, as feature_rows or the step's last update writes
 // it) and the element means (the neighbour part is formed from them)
 int indicator_flags(spdk_mlp* m, const uint16_t* feat, const float2* means, int D, int p, const int N[3],
-                    const int bc[3], long long E, uint8_t* flags, float thr, cudaStream_t s);
+                    const int bc[3], long long E, uint8_t* flags, float thr, cudaStream_t s,
+                    const int* gate = nullptr);
 int mlp_n_in(const spdk_mlp* m);
 
 }  // namespace spdk

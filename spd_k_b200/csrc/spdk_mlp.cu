@@ -673,7 +673,9 @@ __global__ void __launch_bounds__(kTcWarps * 32) k_indicator_rows_tc(const uint1
                                                                      const float2* __restrict__ mean, FeatureGeom F,
                                                                      int n_in, const uint16_t* __restrict__ wbf,
                                                                      const float* __restrict__ z0,
-                                                                     uint8_t* __restrict__ flags, float thr) {
+                                                                     uint8_t* __restrict__ flags, float thr,
+                                                                     const int* gate) {
+    if (gate && *gate) return;  // the solver's device time loop has ended
     extern __shared__ __align__(16) unsigned char sm[];
     const Layout L = layout(n_in);
     const TcSmem S = tc_smem(n_in, kTcWarps);
@@ -795,11 +797,11 @@ int feature_rows(const void* u, bool fp32, int D, int p, const int N[3], const i
 }
 
 int indicator_flags(spdk_mlp* m, const uint16_t* feat, const float2* means, int D, int p, const int N[3],
-                    const int bc[3], long long E, uint8_t* flags, float thr, cudaStream_t s) {
+                    const int bc[3], long long E, uint8_t* flags, float thr, cudaStream_t s, const int* gate) {
     const FeatureGeom F = geom(D, p, N, bc, E);
     if (2 * F.NPT + 4 * D != m->n_in) return fail(SPDK_E_ARG, "indicator input width does not match the solver");
     k_indicator_rows_tc<<<tc_blocks(E), kTcWarps * 32, m->tc_smem, s>>>(feat, means, F, m->n_in, m->wbf, m->z0, flags,
-                                                                        thr);
+                                                                        thr, gate);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? 0 : fail(SPDK_E_CUDA, std::string("indicator: ") + cudaGetErrorString(e));
 }
