@@ -357,6 +357,7 @@ template <typename R, int D, int P, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(kThreads, kDetectBlocksPerSM<D>) fv_detect_kernel(DevGrid G, const double2* __restrict__ rpo,
                                                             const double2* __restrict__ rpn,
                                                             uint8_t* __restrict__ T, int* any_trouble) {
+    pdl_wait();
     if (gate_closed(G)) return;
     fv_detect_kernel_body<R, D, P, TX, TY, TZ>(G, rpo, rpn, T, any_trouble, blockIdx.x);
 }
@@ -836,6 +837,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D>) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+    pdl_wait();
     if (gate_closed(G)) return;
     fv_update_kernel_body<R, D, P, TX, TY, TZ>(G, M, A, blockIdx.x);
 }

@@ -76,6 +76,24 @@ void prof_end(spdk_hydro* h, int kind) {
     h->ev_used += 2;
 }
 
+// a launch of one of the step's kernels with programmatic stream
+// serialization: it may be scheduled while the previous kernel on the stream
+// drains, and waits (pdl_wait) before it reads anything
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 unsigned grid_blocks(const spdk_hydro* h) {
     long long b = 1;
     for (int d = 0; d < h->D; d++) b *= h->G.N[d] / h->tile[d];
@@ -88,8 +106,8 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
     const unsigned blocks = grid_blocks(h);
     int launches = 0;
     // viscous face fluxes of a pass's input, written just before the pass
-    auto viscous = [&](PicardArgsT<R>& A) {
-        if (!h->vg[0]) return;
+    auto viscous = [&](PicardArgsT<R>& A) -> int {
+        if (!h->vg[0]) return 0;
         ViscArgsT<R> V{};
         V.ua_in = A.ua_in;
         V.in_slices = A.in_slices;
@@ -99,9 +117,10 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
         }
         const dim3 grid((unsigned)h->E, (unsigned)(A.in_slices > 1 ? h->nt : 1));
         prof_begin(h);
-        k.visc<<<grid, kViscThreads, 0, h->stream>>>(h->G, dm, V);
+        SPDK_CUDA(launch_pdl(k.visc, grid, dim3(kViscThreads), 0, h->stream, h->G, dm, V));
         prof_end(h, SPDK_KERNEL_OTHER);
         launches++;
+        return 0;
     };
     R* const ua[2] = {(R*)h->ua[0], (R*)h->ua[1]};
     R* const ucv[2] = {(R*)h->ucv[0], (R*)h->ucv[1]};
@@ -127,9 +146,9 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             A.ua_in = in;
             A.in_slices = in_slices;
             A.ua_out = ua[it % 2];
-            viscous(A);
+            if (int rc = viscous(A)) return rc;
             prof_begin(h);
-            k.predict<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
+            SPDK_CUDA(launch_pdl(k.predict, dim3(blocks), dim3(kThreads), k.picard_smem, h->stream, h->G, dm, A));
             prof_end(h, SPDK_KERNEL_PREDICT);
             launches++;
             in = ua[it % 2];
@@ -137,7 +156,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
         }
         A.ua_in = in;
         A.in_slices = in_slices;
-        viscous(A);
+        if (int rc = viscous(A)) return rc;
         if (!h->cfg.fallback) {
             A.u_out = (R*)h->u;
             A.u0 = (const R*)h->u0;
@@ -146,7 +165,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             A.wcv = (R*)h->wcv;
             A.dtmin = h->dtmin;
             prof_begin(h);
-            k.correct<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
+            SPDK_CUDA(launch_pdl(k.correct, dim3(blocks), dim3(kThreads), k.picard_smem, h->stream, h->G, dm, A));
             prof_end(h, SPDK_KERNEL_CORRECT);
             launches++;
         } else {
@@ -155,7 +174,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             A.rp_old = h->rpo;
             A.rp_new = h->rpn;
             prof_begin(h);
-            k.flux<<<blocks, kThreads, k.picard_smem, h->stream>>>(h->G, dm, A);
+            SPDK_CUDA(launch_pdl(k.flux, dim3(blocks), dim3(kThreads), k.picard_smem, h->stream, h->G, dm, A));
             prof_end(h, SPDK_KERNEL_FLUX);
             launches++;
             if (h->join_pending) {
@@ -164,7 +183,8 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             }
             for (int t = 0; t < h->nt; t++) {
                 prof_begin(h);
-                k.detect<<<blocks, kThreads, 0, h->stream>>>(h->G, h->rpo, h->rpn, h->trouble, nullptr);
+                SPDK_CUDA(launch_pdl(k.detect, dim3(blocks), dim3(kThreads), 0, h->stream, h->G,
+                                     (const double2*)h->rpo, (const double2*)h->rpn, h->trouble, (int*)nullptr));
                 prof_end(h, SPDK_KERNEL_DETECT);
                 FallbackArgsT<R> F{};
                 F.ucv_in = ucv[t % 2];
@@ -193,15 +213,17 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
                     F.n_in = 2 * h->NPT + 4 * h->D;
                 }
                 prof_begin(h);
-                k.update<<<blocks, kThreads, k.update_smem, h->stream>>>(h->G, dm, F);
+                SPDK_CUDA(launch_pdl(k.update, dim3(blocks), dim3(kThreads), k.update_smem, h->stream, h->G, dm, F));
                 prof_end(h, SPDK_KERNEL_UPDATE);
                 launches += 2;
             }
         }
     }
     prof_begin(h);
-    if (h->evolve_mode) evolve_advance_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap, h->tb, h->gate);
-    else advance_dt_kernel<<<1, 1, 0, h->stream>>>(h->dt, h->dtmin, h->dt_cap);
+    if (h->evolve_mode)
+        SPDK_CUDA(launch_pdl(evolve_advance_kernel, dim3(1), dim3(1), 0, h->stream, h->dt, h->dtmin, h->dt_cap, h->tb,
+                             h->gate));
+    else SPDK_CUDA(launch_pdl(advance_dt_kernel, dim3(1), dim3(1), 0, h->stream, h->dt, h->dtmin, h->dt_cap));
     prof_end(h, SPDK_KERNEL_OTHER);
     launches++;
     h->launches = launches;

@@ -70,6 +70,13 @@ struct DevGrid {
 
 __device__ __forceinline__ bool gate_closed(const DevGrid& G) { return G.gate && *G.gate; }
 
+// Programmatic dependent launch: a step's kernels are launched with
+// programmatic stream serialization, so a kernel may be scheduled while its
+// predecessor drains; it waits here, before touching any memory, until the
+// predecessor has completed and its writes are visible (a no-op for a
+// normal launch)
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 enum { kPredict = 0, kCorrect = 1, kFlux = 2 };
 
 template <typename R>
@@ -984,6 +991,7 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
 // the inviscid kernels carry none of that code
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
 __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+    pdl_wait();
     if (gate_closed(G)) return;
     picard_kernel_body<R, D, P, TX, TY, TZ, MODE, VISC>(G, M, A, blockIdx.x);
 }

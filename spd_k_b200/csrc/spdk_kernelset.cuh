@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(kThreads) derive_kernel(DevGrid G, DevMatsT<R>
 // cap > 0 (src/hydro.cpp:245-254: every point's candidate is min(dt, cap),
 // so the minimum over points is min(reduced, cap)); re-arm the reduction
 static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin, double cap) {
+    pdl_wait();
     const double v = __longlong_as_double((long long)*dtmin);
     *dt = (cap > 0.0 && !(v < cap)) ? cap : v;
     *dtmin = 0x7FEFFFFFFFFFFFFFULL;
@@ -99,6 +100,7 @@ static __global__ void advance_dt_kernel(double* dt, unsigned long long* dtmin, 
 // FP64 operations as the host loop, so the dt sequence is identical.
 static __global__ void evolve_advance_kernel(double* dt, unsigned long long* dtmin, double cap, double* tb,
                                              int* gate) {
+    pdl_wait();
     if (*gate) return;
     const double used = *dt;
     const double v = __longlong_as_double((long long)*dtmin);
@@ -119,6 +121,7 @@ static __global__ void evolve_advance_kernel(double* dt, unsigned long long* dtm
 
 // per-element trouble labels of a step <- 0 (skipped once the gate is closed)
 static __global__ void clear_labels_kernel(DevGrid G, uint8_t* labels, long long n) {
+    pdl_wait();
     if (gate_closed(G)) return;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         labels[i] = 0;

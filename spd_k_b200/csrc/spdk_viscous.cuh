@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
     __shared__ R dU[D * D * NPT];              // [e][momentum][point] gradients
     __shared__ R Msf[nf * n], Mdf[n * nf];
 
+    pdl_wait();
     if (gate_closed(G)) return;
     const int tid = threadIdx.x;
     const long long ge = blockIdx.x;
