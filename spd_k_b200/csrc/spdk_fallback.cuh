@@ -521,9 +521,11 @@ __device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], in
 
 // resident blocks the update kernel is compiled for: 5 (48 registers) in 2D,
 // where the extra warps hide its gather latency (measured on B200 at 256^2,
-// p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64)
+// p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64); 2 in 3D
+// (128 registers, no spills; at 1 block the 140-register kernel left one
+// block per SM: 3D 32^3 p=3 step 21.1 -> 15.5 ms in FP64)
 template <int D>
-constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : 1;
+constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : 2;
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
 struct UpdateSmem {
