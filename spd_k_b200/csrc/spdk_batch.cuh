@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(kThreads, kDetectBlocksPerSM<D>) detect_batche
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D>)
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D, P>)
     update_batched(const BatchItem<FallbackArgsT<R>>* __restrict__ items, int n, DevMatsT<R> M) {
     long long b;
     const BatchItem<FallbackArgsT<R>>& it = batch_item(items, n, &b);

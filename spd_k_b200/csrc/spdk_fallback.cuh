@@ -521,11 +521,12 @@ __device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], in
 
 // resident blocks the update kernel is compiled for: 5 (48 registers) in 2D,
 // where the extra warps hide its gather latency (measured on B200 at 256^2,
-// p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64); 2 in 3D
-// (128 registers, no spills; at 1 block the 140-register kernel left one
-// block per SM: 3D 32^3 p=3 step 21.1 -> 15.5 ms in FP64)
-template <int D>
-constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : 2;
+// p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64). In 3D
+// (one element per block) the 140-register kernel ran one block per SM;
+// measured per step of 4 updates, FP64: 32^3 p=3 6.15 / 3.47 / 2.52 ms at
+// 2 / 3 / 4 blocks, 16^3 p=5 4.13 / 3.65 / 4.05 ms
+template <int D, int P>
+constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : (P <= 3 ? 4 : 3);
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
 struct UpdateSmem {
@@ -838,7 +839,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D>) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D, P>) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
     pdl_wait();
     if (gate_closed(G)) return;
     fv_update_kernel_body<R, D, P, TX, TY, TZ>(G, M, A, blockIdx.x);
