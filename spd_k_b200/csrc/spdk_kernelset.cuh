@@ -176,9 +176,13 @@ bool pick2(int Nx, int Ny, KernelSetT<R>* k, bool visc) {
     *k = make_set<R, 2, P, 1, 1, 1>();
     return true;
 }
+// 3D: one element per tile, or 2x1x1 elements at p <= 3, where one
+// element's (p+1)^3 points would leave most of the block idle in the
+// per-point phases
 template <typename R, int P>
-bool pick3(int, int, int, KernelSetT<R>* k, bool visc) {
+bool pick3(int Nx, int, int, KernelSetT<R>* k, bool visc) {
     if (visc) *k = make_set<R, 3, P, 1, 1, 1, true>();
+    else if (P <= 3 && Nx % 2 == 0) *k = make_set<R, 3, P, 2, 1, 1>();
     else *k = make_set<R, 3, P, 1, 1, 1>();
     return true;
 }

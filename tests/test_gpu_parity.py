@@ -137,6 +137,10 @@ RANDOM_CASES = {
                        "mesh/x3_bc=reflective"],
     "3d_p3_rk2": ["job/fallback=false", "mesh/nx1=2", "mesh/nx2=3", "mesh/nx3=2", "time/integrator=rk2",
                   "hydro/g3=0.3"],
+    # 3D tiles of 2x1x1 elements (p <= 3, even nx1), with the fallback
+    "3d_p3_fallback_tile2": ["job/fallback=true", "mesh/nx1=2", "mesh/nx2=3", "mesh/nx3=2", "mesh/x2_bc=reflective"],
+    "3d_p2_fallback_tile2": ["job/fallback=true", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=3", "mesh/nx3=2",
+                             "mesh/x1_bc=gradfree"],
     # viscous terms on every boundary kind, ADER and SSP-RK, with the fallback
     "2d_p3_viscous_fallback_reflective": ["job/fallback=true", "mesh/nx1=6", "mesh/nx2=4", "mesh/nx3=1",
                                           "mesh/x1_bc=reflective", "mesh/x2_bc=gradfree", "hydro/nu=0.02"],
