@@ -528,10 +528,15 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // keeps no per-slice registers and takes one block more at p = 3 in 2D
 // (FP32 5 blocks: 159 against 167 us; FP64 3 blocks: 338 against 376 us);
 // the predictor and corrector spill heavily there.
+// In 3D at p = 5 the FP64 passes' 161 KB of shared memory admit one block
+// per SM anyway, so they take the whole register file instead of spilling
+// at 128 registers.
 template <typename R, int D, int P, int MODE>
 constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
                                        ? (P == 3 ? (MODE == kFlux ? 5 : 4) : 3)
-                                       : (MODE == kFlux && D == 2 && P == 3 ? 3 : 2);
+                                       : (sizeof(R) == 8 && D == 3 && P >= 5)
+                                             ? 1
+                                             : (MODE == kFlux && D == 2 && P == 3 ? 3 : 2);
 
 // flux-point buffers of a Picard pass (alternated between slices when 2)
 template <typename R>
