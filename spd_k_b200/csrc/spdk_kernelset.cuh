@@ -165,16 +165,19 @@ KernelSetT<R> make_set() {
 }
 
 // Tile choice: the largest instantiated tile that divides the element counts.
-// Viscous runs (visc) take the one-element tile with the viscous Picard passes.
+// Viscous runs (VISC) take the same tiles with the viscous Picard passes.
+template <typename R, int P, bool VISC>
+bool pick2_t(int Nx, int Ny, KernelSetT<R>* k) {
+    if constexpr (P <= 4) {
+        if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<R, 2, P, 4, 4, 1, VISC>(); return true; }
+    }
+    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<R, 2, P, 2, 2, 1, VISC>(); return true; }
+    *k = make_set<R, 2, P, 1, 1, 1, VISC>();
+    return true;
+}
 template <typename R, int P>
 bool pick2(int Nx, int Ny, KernelSetT<R>* k, bool visc) {
-    if (visc) { *k = make_set<R, 2, P, 1, 1, 1, true>(); return true; }
-    if constexpr (P <= 4) {
-        if (Nx % 4 == 0 && Ny % 4 == 0) { *k = make_set<R, 2, P, 4, 4, 1>(); return true; }
-    }
-    if (Nx % 2 == 0 && Ny % 2 == 0) { *k = make_set<R, 2, P, 2, 2, 1>(); return true; }
-    *k = make_set<R, 2, P, 1, 1, 1>();
-    return true;
+    return visc ? pick2_t<R, P, true>(Nx, Ny, k) : pick2_t<R, P, false>(Nx, Ny, k);
 }
 // 3D: one element per tile, or 2x1x1 elements at p <= 3, where one
 // element's (p+1)^3 points would leave most of the block idle in the
