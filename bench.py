@@ -318,6 +318,48 @@ def batched_leg(args, local, dist, world, rank=0):
     return res
 
 
+def kernel_profile(L, solver, steps, esz, workload):
+    """per-kernel CUDA-event times of `steps` steps launched one by one with
+    an event pair around every launch (no graph), the algorithmic GB/s of
+    each kernel kind, and the roofline of the dominant kind"""
+    import ctypes
+    from spd_k_b200.api import _lib
+    L.spdk_hydro_profile.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_longlong)]
+    kms = (ctypes.c_double * 7)()
+    kl = (ctypes.c_longlong * 7)()
+    rc = L.spdk_hydro_profile(solver.h, steps, kms, kl)
+    assert rc == 0, _lib.spdk_last_error()
+    per_kind = {KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i]),
+                           "avg_us": (1e3 * kms[i] / kl[i]) if kl[i] else None} for i in range(7)}
+    info = solver.info
+    alg = algorithmic_bytes(info, True, esz)
+    dom = max((k for k in KINDS if k in alg and per_kind[k]["launches"]), key=lambda k: per_kind[k]["ms"])
+    hbm, peak_kind = peaks()
+    achieved = alg[dom] / (per_kind[dom]["avg_us"] * 1e-6) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic_from_profiles(dom, workload),
+                "algorithmic_bytes": alg[dom]}
+    table = {k: dict(v, algorithmic_gbs=(alg[k] / (v["avg_us"] * 1e-6) / 1e9 if k in alg and v["avg_us"] else None),
+                     hbm_frac=(alg[k] / (v["avg_us"] * 1e-6) / 1e9 / hbm if k in alg and v["avg_us"] else None))
+             for k, v in per_kind.items() if v["launches"]}
+    table["note"] = (f"{steps} steps launched one by one with a CUDA-event pair around each launch (no graph, "
+                     "no overlap between launches): the sum over kinds exceeds the graph-replayed step time")
+    return table, roofline
+
+
+def mid_run_state(c, t_mid, local):
+    """the plain FP64 run's state at t_mid (first step end at or after it),
+    stepped on the device by the time loop: (U_sp as doubles, t, steps)"""
+    import spd_k_b200 as S
+    sv = S.HydroSolver(dict(c, precision="fp64"), device=local)
+    n = sv.evolve(t_mid)
+    u = sv.read(S.FIELD_U_SP)
+    t = sv.t
+    sv.close()
+    return u, t, n
+
+
 def run_reference_arm(args):
     rank, world, local, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
                                 int(os.environ.get("LOCAL_RANK", "0")), None)
@@ -358,6 +400,8 @@ def main():
     ap.add_argument("--batch-problems", type=int, default=512,
                     help="problems of the batched-ensemble leg (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--t-mid", type=float, default=0.025,
+                    help="simulated time of the state the steps are timed from (0: the initial blast)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -380,7 +424,16 @@ def main():
         import torch
         torch.cuda.set_device(local)
         ind = Indicator.load(args.learned)
+    # the state the steps are timed from: the plain FP64 run at t_mid, where
+    # the blast's shock ring keeps the fallback busy (untimed set-up)
+    u_mid, t_mid, mid_steps = (None, 0.0, 0)
+    if args.t_mid > 0:
+        import torch
+        torch.cuda.set_device(local)
+        u_mid, t_mid, mid_steps = mid_run_state(c, args.t_mid, local)
     solver = S.HydroSolver(c, device=local)
+    if u_mid is not None:
+        solver.write_u(u_mid)
     if ind is not None:
         set_indicator(solver, ind, args.threshold)
     L = S.load_library()
@@ -428,25 +481,8 @@ def main():
     value = aggregate_throughput(world, dof, args.steps, ms)
 
     # ---- per-kernel CUDA-event pass (same stream, no graph) ----
-    L.spdk_hydro_profile.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
-                                     ctypes.POINTER(ctypes.c_longlong)]
-    kms = (ctypes.c_double * 7)()
-    kl = (ctypes.c_longlong * 7)()
-    rc = L.spdk_hydro_profile(solver.h, args.profile_steps, kms, kl)
-    assert rc == 0, _lib.spdk_last_error()
-    per_kind = {KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i]),
-                           "avg_us": (1e3 * kms[i] / kl[i]) if kl[i] else None} for i in range(7)}
-    alg = algorithmic_bytes(info, c["fallback"], esz)
-    dom = max((k for k in KINDS if k in alg and per_kind[k]["launches"]), key=lambda k: per_kind[k]["ms"])
-    hbm, peak_kind = peaks()
-    achieved = alg[dom] / (per_kind[dom]["avg_us"] * 1e-6) / 1e9
-    traffic = traffic_from_profiles(dom, WORKLOAD if args.precision == "fp64" else f"{WORKLOAD}-{args.precision}")
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes": alg[dom]}
-    kernel_table = {k: dict(v, algorithmic_gbs=(alg[k] / (v["avg_us"] * 1e-6) / 1e9
-                                                 if k in alg and v["avg_us"] else None))
-                    for k, v in per_kind.items() if v["launches"]}
+    kernel_table, roofline = kernel_profile(
+        L, solver, args.profile_steps, esz, WORKLOAD if args.precision == "fp64" else f"{WORKLOAD}-{args.precision}")
 
     # ---- e2e through the C ABI with host buffers (reference driver loop) ----
     solver2 = S.HydroSolver(c, device=local)
@@ -454,15 +490,19 @@ def main():
         set_indicator(solver2, ind, args.threshold)
     u_host = torch.empty(info.n_elements * info.nvar * info.n_points, dtype=torch.float64,
                          pin_memory=True).numpy()   # the C ABI exchanges doubles in both forms
-    solver2.read(S.FIELD_U_SP, out=u_host)
+    if u_mid is not None:
+        u_host[:] = u_mid
+    else:
+        solver2.read(S.FIELD_U_SP, out=u_host)
     w_host = torch.empty_like(torch.from_numpy(u_host)).pin_memory().numpy()
     rc = L.spdk_hydro_get_stream(solver2.h, ctypes.byref(sp))
     stream2 = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
     e2e_steps = max(1, min(args.steps, 200))
-    # simulated time the job runs to: the sum of the dts of e2e_steps steps
-    # from the written state (untimed; the timed run repeats the same dts)
+    # simulated time the job runs to: t_mid plus the sum of the dts of
+    # e2e_steps steps from the written state (untimed; the timed run repeats
+    # the same dts)
     solver2.write_u(u_host)
-    t_end = 0.0
+    t_end = t_mid
     dt = solver2.dt()
     for _ in range(e2e_steps):
         solver2.step()
@@ -488,21 +528,26 @@ def main():
             solver2.dt()                        # blocking D2H of the step's dt (the reference's loop)
         return e2e_steps
 
-    # time_evolution through the C ABI (spdk_hydro_evolve: the loop on the device)
-    n_evolve, e2e_ms = timed(lambda: solver2.evolve(t_end))
+    # time_evolution through the C ABI (spdk_hydro_evolve_from: the loop on
+    # the device, resumed at t_mid)
+    n_evolve, e2e_ms = timed(lambda: solver2.evolve(t_end, t0=t_mid))
     n_loop, loop_ms = timed(per_step)
     state_bytes = u_host.nbytes
     e2e = {"value": world * dof * n_evolve / (e2e_ms * 1e-3), "unit": "DOF-updates/s",
            "h2d_bytes_per_step": state_bytes / n_evolve, "d2h_bytes_per_step": state_bytes / n_evolve,
-           "steps": n_evolve, "t_end": t_end,
-           "path": "spdk_hydro_write + spdk_hydro_evolve(t_end) + spdk_hydro_read",
+           "steps": n_evolve, "t0": t_mid, "t_end": t_end,
+           "path": "spdk_hydro_write + spdk_hydro_evolve_from(t_mid, t_end) + spdk_hydro_read",
            "host_step_loop": {"value": world * dof * n_loop / (loop_ms * 1e-3),
                               "path": "spdk_hydro_step + blocking spdk_hydro_get_dt per step"}}
     solver2.close()
 
     # ---- the other forms on the same workload, beside the timed one ----
-    def time_form(cf):
+    def time_form(cf, u0=u_mid, profile=False, with_ind=False):
         sv = S.HydroSolver(cf, device=local)
+        if u0 is not None:
+            sv.write_u(u0)
+        if with_ind:
+            set_indicator(sv, ind, args.threshold)
         rc = L.spdk_hydro_get_stream(sv.h, ctypes.byref(sp))
         st = torch.cuda.ExternalStream(sp.value, device=f"cuda:{local}")
         sv.steps(args.warmup)
@@ -515,12 +560,28 @@ def main():
         g1.record(st)
         g1.synchronize()
         msf = max_over_ranks(dist, g0.elapsed_time(g1), f"cuda:{local}")
+        res = {"value": aggregate_throughput(world, dof, args.steps, msf), "unit": "DOF-updates/s",
+               "ms_per_step": msf / args.steps, "steps": args.steps,
+               "timed_form_speedup": (msf / args.steps) / (ms / args.steps)}
+        if profile:
+            esz_f = 4 if cf["precision"] == "fp32" else 8
+            wl = WORKLOAD if cf["precision"] == "fp64" else f"{WORKLOAD}-{cf['precision']}"
+            res["kernels"], res["roofline"] = kernel_profile(L, sv, args.profile_steps, esz_f, wl)
+        if with_ind:
+            set_indicator(sv, None)
         sv.close()
-        return {"value": aggregate_throughput(world, dof, args.steps, msf), "unit": "DOF-updates/s",
-                "ms_per_step": msf / args.steps, "steps": args.steps,
-                "timed_form_speedup": (msf / args.steps) / (ms / args.steps)}
-    plain = time_form(dict(c, precision="fp64")) if (args.precision != "fp64" or learned) else None
+        return res
+    plain = time_form(dict(c, precision="fp64"), profile=True) if (args.precision != "fp64" or learned) else None
     mixed = time_form(dict(c, precision="fp32")) if (args.precision == "fp32" and learned) else None
+    # the same forms timed from the initial blast (t = 0), where the shock
+    # is small and the fallback nearly idle
+    initial = None
+    if u_mid is not None:
+        initial = {"state": "t = 0, the initial blast",
+                   "timed_form": dict(time_form(dict(c), u0=None, with_ind=learned), form=form),
+                   "plain_fp64": time_form(dict(c, precision="fp64"), u0=None)}
+        if args.precision == "fp32" and learned:
+            initial["mixed_without_indicator"] = time_form(dict(c, precision="fp32"), u0=None)
 
     # ---- batched ensemble: independent four-quadrant Riemann problems ----
     batched = None
@@ -556,13 +617,17 @@ def main():
                                              if learned else None),
                        "parallelism": f"replicas{world}",
                        "l2": f"no flush: device working set {state_gb:.2f} GB > 126 MB L2",
-                       "state": "steps continue from the initial blast after the warm-up"},
+                       "state": (f"mid-run: the plain FP64 run's state at t = {t_mid:.6g} ({mid_steps} steps "
+                                 f"from the initial blast, untimed), then {args.warmup} warm-up steps"
+                                 if u_mid is not None else
+                                 "steps continue from the initial blast after the warm-up")},
             "gpu_launches": info.launches_per_step * args.steps,
             "roofline": roofline,
             "kernels": kernel_table,
             "e2e": e2e,
             "plain_fp64": plain,
             "mixed_without_indicator": mixed,
+            "initial_state": initial,
             "batched": batched,
             "cpu_baseline": cpu,
             "clocks": clk,

@@ -142,8 +142,15 @@ int spdk_hydro_steps(spdk_hydro* h, int n);
  * next dt and closes a stop gate at t_end (the host loop's FP64 operations,
  * so the steps and states equal a host loop's bit for bit); the host
  * launches captured steps in batches and reads the loop state once per
- * batch. Steps launched past the gate do nothing. */
+ * batch. Steps launched past the gate do nothing. The loop starts at t = 0
+ * with the first output time dt_output, as a fresh run does. */
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t);
+/* the same loop resumed at t0 with the next output time t_output0 (ignored
+ * when dt_output <= 0): after spdk_hydro_restore, pass the checkpoint's t and
+ * t_output from spdk_checkpoint_info to continue the interrupted run. *t
+ * receives the final time (t0 when t0 >= t_end: no step is taken). */
+int spdk_hydro_evolve_from(spdk_hydro* h, double t0, double t_output0, double t_end, double dt_output,
+                           long long* steps, double* t);
 int spdk_hydro_sync(spdk_hydro* h);
 /* the CUDA stream (cudaStream_t) every solver launch is ordered on */
 int spdk_hydro_get_stream(spdk_hydro* h, void** stream);
@@ -243,10 +250,21 @@ int spdk_fv_faces(int N, int p, double L, int active, double* out, size_t count)
  * are rejected with SPDK_E_ARG. The first call on a device, with that device
  * current, resolves the array's device address and sets kernel attributes:
  * make it before any stream capture. Calls share the array, so calls that
- * overlap on the GPU race; order them on one stream. No call allocates. */
+ * overlap on the GPU race; order them on one stream. No call allocates.
+ * Slab configurations (slab_lo, slab_n != 0) are rejected with SPDK_E_ARG.
+ * Device-detected faults: every call clears the array's status word when it
+ * starts; if a bounded shared-memory staging wait runs out during the call,
+ * *dt_inout receives NaN instead of the next dt (the state it leaves is not
+ * to be trusted) and the status word keeps the fault bit. */
 #define SPDK_NOALLOC_SCRATCH_BYTES (16u << 20)
 int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const double* u_in, double* u_out, double* wcv_out,
                             double* dt_inout, void* stream);
+/* Status word of the last spdk_hydro_step_noalloc call on the current
+ * device: 0 = clean, bit 0 (value 1) = a staging wait timed out. Blocking:
+ * it reads the word on `stream` (a cudaStream_t; order it after the step)
+ * and waits for that stream. 0 when no step ran on the device yet. No
+ * counterpart in the reference; allocates nothing. */
+int spdk_hydro_noalloc_status(int* status_out, void* stream);
 
 #ifdef __cplusplus
 }

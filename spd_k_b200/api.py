@@ -88,7 +88,7 @@ class CheckpointInfo(ctypes.Structure):
 EXPORTS = (
     "spdk_last_error", "spdk_abi_version", "spdk_hydro_create", "spdk_hydro_destroy",
     "spdk_hydro_get_info", "spdk_hydro_get_dt", "spdk_hydro_set_dt", "spdk_hydro_step",
-    "spdk_hydro_steps", "spdk_hydro_evolve", "spdk_hydro_sync", "spdk_hydro_read",
+    "spdk_hydro_steps", "spdk_hydro_evolve", "spdk_hydro_evolve_from", "spdk_hydro_sync", "spdk_hydro_read",
     "spdk_hydro_write",
 )
 
@@ -118,6 +118,9 @@ def load_library(path=LIB_PATH):
     L.spdk_hydro_steps.argtypes = [ctypes.c_void_p, ctypes.c_int]
     L.spdk_hydro_evolve.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
+    L.spdk_hydro_evolve_from.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_double)]
     L.spdk_hydro_sync.argtypes = [ctypes.c_void_p]
     L.spdk_hydro_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.c_size_t]
@@ -341,9 +344,16 @@ class HydroSolver:
     def sync(self):
         _check(_lib.spdk_hydro_sync(self.h))
 
-    def evolve(self, t_end, dt_output=None):
+    def evolve(self, t_end, dt_output=None, t0=None, t_output=None):
+        """time_evolution on the device (spdk_hydro_evolve); with t0 (and the
+        next output time t_output) it resumes a run (spdk_hydro_evolve_from)"""
         steps, t = ctypes.c_longlong(), ctypes.c_double()
-        _check(_lib.spdk_hydro_evolve(self.h, t_end, dt_output or -1.0, ctypes.byref(steps), ctypes.byref(t)))
+        if t0 is None:
+            _check(_lib.spdk_hydro_evolve(self.h, t_end, dt_output or -1.0, ctypes.byref(steps), ctypes.byref(t)))
+        else:
+            t_out0 = t_output if t_output is not None else -1.0
+            _check(_lib.spdk_hydro_evolve_from(self.h, t0, t_out0, t_end, dt_output or -1.0, ctypes.byref(steps),
+                                               ctypes.byref(t)))
         self.t = t.value
         self.n_step += steps.value
         return steps.value
@@ -406,6 +416,7 @@ class HydroSolver:
                 if self.t + dt > t_output:
                     dt = t_output - self.t
                     self.set_dt(dt)
+        self.t_output = t_output
         return dt
 
     # ---- layout helpers -------------------------------------------------

@@ -31,7 +31,9 @@ int fail(int code, const std::string& msg);
 namespace {
 
 constexpr char kMagic[8] = {'S', 'P', 'D', 'K', 'C', 'K', 'P', '1'};
-constexpr uint32_t kVersion = 1;
+// version 2 adds the geometry and physics fields after cfl; version 1 files
+// (those fields zero) are still read, with the version-1 checks only
+constexpr uint32_t kVersion = 2;
 
 // 256 bytes, little-endian, naturally aligned
 struct CkptHeader {
@@ -41,7 +43,10 @@ struct CkptHeader {
     double t, dt, t_output;
     int64_t steps, outputs;
     double gamma, cfl;
-    uint8_t reserved[112];
+    // version 2: box lengths, gravity, viscosity, fallback settings, slab
+    double L[3], g[3], nu, beta, nad_tolerance;
+    int32_t nad_delta, nad_moore, sed, blending, slab_lo, slab_n;
+    uint8_t reserved[16];
 };
 static_assert(sizeof(CkptHeader) == 256, "checkpoint header layout");
 
@@ -70,6 +75,19 @@ CkptHeader make_header(const spdk_hydro* h, const spdk_checkpoint_info& info) {
     hd.outputs = info.outputs;
     hd.gamma = h->cfg.gamma;
     hd.cfl = h->cfg.cfl;
+    for (int d = 0; d < 3; d++) {
+        hd.L[d] = h->cfg.L[d];
+        hd.g[d] = h->cfg.g[d];
+    }
+    hd.nu = h->cfg.nu;
+    hd.beta = h->cfg.beta;
+    hd.nad_tolerance = h->cfg.nad_tolerance;
+    hd.nad_delta = h->cfg.nad_delta;
+    hd.nad_moore = h->cfg.nad_moore;
+    hd.sed = h->cfg.sed;
+    hd.blending = h->cfg.blending;
+    hd.slab_lo = h->cfg.slab_lo;
+    hd.slab_n = h->cfg.slab_n;
     return hd;
 }
 
@@ -100,7 +118,7 @@ bool write_ckpt(const std::string& path, const CkptHeader& hd, const void* data,
 int read_header(FILE* f, const char* path, CkptHeader* hd) {
     if (std::fread(hd, sizeof(*hd), 1, f) != 1) return fail(SPDK_E_IO, std::string("short checkpoint header in ") + path);
     if (std::memcmp(hd->magic, kMagic, 8) != 0) return fail(SPDK_E_ARG, std::string(path) + " is not a checkpoint");
-    if (hd->version != kVersion)
+    if (hd->version != 1 && hd->version != kVersion)
         return fail(SPDK_E_ARG, "checkpoint version " + std::to_string(hd->version) + " is not supported");
     return 0;
 }
@@ -219,6 +237,14 @@ int spdk_hydro_restore(spdk_hydro* h, const char* path, spdk_checkpoint_info* in
                     hd.fallback == mine.fallback && hd.esz == mine.esz && hd.count == mine.count &&
                     hd.gamma == mine.gamma && hd.cfl == mine.cfl;
         for (int d = 0; d < 3; d++) same = same && hd.N[d] == mine.N[d] && hd.bc[d] == mine.bc[d];
+        if (hd.version >= 2) {
+            // geometry and physics: a state of another box, gravity, viscosity,
+            // fallback setting or slab would restore silently and diverge
+            for (int d = 0; d < 3; d++) same = same && hd.L[d] == mine.L[d] && hd.g[d] == mine.g[d];
+            same = same && hd.nu == mine.nu && hd.beta == mine.beta && hd.nad_tolerance == mine.nad_tolerance &&
+                   hd.nad_delta == mine.nad_delta && hd.nad_moore == mine.nad_moore && hd.sed == mine.sed &&
+                   hd.blending == mine.blending && hd.slab_lo == mine.slab_lo && hd.slab_n == mine.slab_n;
+        }
         if (!same) rc = fail(SPDK_E_ARG, std::string(path) + " was written by a solver of another configuration");
     }
     std::vector<unsigned char> buf;

@@ -661,6 +661,11 @@ int spdk_hydro_sync(spdk_hydro* h) {
 }
 
 int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* steps, double* t_out) {
+    return spdk_hydro_evolve_from(h, 0.0, dt_output, t_end, dt_output, steps, t_out);
+}
+
+int spdk_hydro_evolve_from(spdk_hydro* h, double t0, double t_output0, double t_end, double dt_output,
+                           long long* steps, double* t_out) {
     if (!h) return fail(SPDK_E_ARG, "null argument");
     // src/hydro_ader.hpp:215-273 as a device-resident loop: the step's dt,
     // t, the output clamping and the stop test live on the device
@@ -669,8 +674,8 @@ int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* 
     // batch instead of once per step. Steps launched after t reaches t_end
     // find the gate closed and do nothing.
     if (steps) *steps = 0;
-    if (t_out) *t_out = 0;
-    if (!(0.0 < t_end)) return 0;
+    if (t_out) *t_out = t0;
+    if (!(t0 < t_end)) return 0;
     if (int rc = refresh_features(h)) return rc;
     if (!h->graph_evolve) {
         cudaGraph_t g;
@@ -688,14 +693,25 @@ int spdk_hydro_evolve(spdk_hydro* h, double t_end, double dt_output, long long* 
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
     }
-    const double tb0[5] = {0.0, dt_output, 0.0, t_end, dt_output > 0 ? dt_output : -1.0};
+    const double tb0[5] = {t0, t_output0, 0.0, t_end, dt_output > 0 ? dt_output : -1.0};
     SPDK_CUDA(cudaMemcpyAsync(h->tb, tb0, sizeof(tb0), cudaMemcpyHostToDevice, h->stream));
     SPDK_CUDA(cudaMemsetAsync(h->gate, 0, sizeof(int), h->stream));
-    double st[3] = {0, 0, 0};
+    // loop state read back after every batch: t, t_output, steps, and the
+    // next dt, from which the next batch's length is estimated as the steps
+    // the remaining time takes at that dt (a shrinking dt needs another
+    // batch; a growing one leaves a few gated no-op replays)
+    double st[3] = {t0, t_output0, 0};
+    double dt_now = 0;
+    SPDK_CUDA(cudaMemcpyAsync(&dt_now, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    SPDK_CUDA(cudaStreamSynchronize(h->stream));
     int closed = 0;
-    for (int batch = 8; !closed; batch = std::min(batch * 2, 64)) {
+    while (!closed) {
+        double est = dt_now > 0 ? std::ceil((t_end - st[0]) / dt_now) : 1.0;
+        if (!(est >= 1.0)) est = 1.0;
+        const int batch = (int)std::min(est, 256.0);
         for (int q = 0; q < batch; q++) SPDK_CUDA(cudaGraphLaunch(h->graph_evolve, h->stream));
         SPDK_CUDA(cudaMemcpyAsync(st, h->tb, sizeof(st), cudaMemcpyDeviceToHost, h->stream));
+        SPDK_CUDA(cudaMemcpyAsync(&dt_now, h->dt, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         SPDK_CUDA(cudaMemcpyAsync(&closed, h->gate, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
         SPDK_CUDA(cudaStreamSynchronize(h->stream));
         if (int rc = check_status(h)) return rc;

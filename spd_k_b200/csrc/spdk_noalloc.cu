@@ -52,11 +52,18 @@ constexpr int kMaxDevices = 64;
 void* g_scratch_ptr[kMaxDevices] = {};
 std::mutex g_setup_mutex;
 
-// dt reduction word <- largest double; re-armed at the start of every call
-__global__ void noalloc_arm(unsigned long long* dtmin) { *dtmin = 0x7FEFFFFFFFFFFFFFULL; }
+// start of every call: dt reduction word <- largest double, status word <- 0
+__global__ void noalloc_arm(unsigned long long* dtmin, int* status) {
+    *dtmin = 0x7FEFFFFFFFFFFFFFULL;
+    *status = 0;
+}
 
-__global__ void noalloc_finish(double* dt, unsigned long long* dtmin) {
-    *dt = __longlong_as_double((long long)*dtmin);
+// end of every call: the next dt, or NaN when a bounded staging wait ran
+// out during the call (the state it leaves is then not to be trusted; the
+// status word keeps the bit for spdk_hydro_noalloc_status)
+__global__ void noalloc_finish(double* dt, unsigned long long* dtmin, const int* status) {
+    *dt = (*status & kStatusStagingTimeout) ? __longlong_as_double(0x7FF8000000000000LL)
+                                            : __longlong_as_double((long long)*dtmin);
     *dtmin = 0x7FEFFFFFFFFFFFFFULL;
 }
 
@@ -96,6 +103,8 @@ extern "C" int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const doubl
     if (c.p < 1 || c.p > kMaxP) return fail(SPDK_E_ARG, "p must be in 1..7");
     if (c.N[0] < 2 || c.N[1] < 2) return fail(SPDK_E_ARG, "x and y must be active (nx1, nx2 > 1)");
     if (c.precision != SPDK_PRECISION_FP64) return fail(SPDK_E_ARG, "unsupported precision");
+    if (c.slab_n != 0 || c.slab_lo != 0)
+        return fail(SPDK_E_ARG, "the allocation-free step steps whole domains: set slab_lo = slab_n = 0");
     const int D = c.N[2] > 1 ? 3 : 2;
     if (D == 3 && c.p > 5) return fail(SPDK_E_ARG, "3D runs support p <= 5");
     if (D == 2 && (c.g[2] != 0.0 || ((c.problem == SPDK_IC_SINE_WAVE || c.problem == SPDK_IC_SQUARE) && c.v3 != 0.0)))
@@ -168,7 +177,7 @@ extern "C" int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const doubl
     cudaStream_t s = (cudaStream_t)stream;
     long long blocks = 1;
     for (int d = 0; d < D; d++) blocks *= N[d] / ks.tile[d];
-    noalloc_arm<<<1, 1, 0, s>>>(dtmin);
+    noalloc_arm<<<1, 1, 0, s>>>(dtmin, status);
     double rk_a[3] = {0, 0, 0};
     if (c.rk_order == 2) rk_a[1] = 0.5;
     if (c.rk_order == 3) { rk_a[1] = 0.75; rk_a[2] = 1.0 / 3.0; }
@@ -219,8 +228,30 @@ extern "C" int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const doubl
             cur = u_out;
         }
     }
-    noalloc_finish<<<1, 1, 0, s>>>(dt_inout, dtmin);
+    noalloc_finish<<<1, 1, 0, s>>>(dt_inout, dtmin, status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+extern "C" int spdk_hydro_noalloc_status(int* status_out, void* stream) {
+    if (!status_out) return fail(SPDK_E_ARG, "null argument");
+    *status_out = 0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(SPDK_E_CUDA, "cudaGetDevice failed");
+    if (dev < 0 || dev >= kMaxDevices) return fail(SPDK_E_ARG, "device ordinal out of range");
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        base = g_scratch_ptr[dev];
+    }
+    if (!base) return 0;  // no step on this device yet: nothing to report
+    cudaStream_t s = (cudaStream_t)stream;
+    int st = 0;
+    cudaError_t e = cudaMemcpyAsync(&st, (char*)base + sizeof(unsigned long long), sizeof(int),
+                                    cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("status read: ") + cudaGetErrorString(e));
+    *status_out = st;
     return 0;
 }

@@ -26,7 +26,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "spd_K_ref")
-REF_TREE = "/root/reference"
+# the reference tree: SPDK_REFERENCE_ROOT, by default where this build keeps it
+REF_TREE = os.environ.get("SPDK_REFERENCE_ROOT", "/root/reference")
 
 BLAST = ["problem/problem=spherical_blast", "hydro/gamma=1.6666666666667"]
 CASES = {

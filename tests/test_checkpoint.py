@@ -23,23 +23,31 @@ from helpers import gpu_config
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "spd_k_b200", "spdk_run")
 
-HEADER = "<8s18IQ3d2q2d112x"   # the 256-byte header of include/spdk.h
+HEADER_V1 = "<8s18IQ3d2q2d112x"   # the 256-byte header, version 1
+# version 2: box lengths, gravity, nu, beta, NAD tolerance, four fallback
+# switches, slab_lo, slab_n
+HEADER_V2 = "<8s18IQ3d2q2d3d3d3d6i16x"
 
 
 def fake_checkpoint(path, magic=b"SPDKCKP1", version=1, t=0.125, t_output=0.25, steps=17, outputs=3):
     ints = [version, 1, 2, 3, 64, 48, 1, 4, 16, 0, 1, 1, 1, 1, 0, 4, 0, 0]
     count = 64 * 48 * 4 * 16
-    hd = struct.pack(HEADER, magic, *ints, count, t, 1e-4, t_output, steps, outputs, 1.4, 0.8)
+    common = (magic, *ints, count, t, 1e-4, t_output, steps, outputs, 1.4, 0.8)
+    if version == 2:
+        hd = struct.pack(HEADER_V2, *common, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 1e-5, 0, 1, 1, 1, 0, 0)
+    else:
+        hd = struct.pack(HEADER_V1, *common)
     assert len(hd) == 256
     with open(path, "wb") as f:
         f.write(hd)
         f.write(np.zeros(count, dtype=np.float32).tobytes())
 
 
-def test_peek_reads_the_header(tmp_path):
+@pytest.mark.parametrize("version", [1, 2])
+def test_peek_reads_the_header(tmp_path, version):
     from spd_k_b200.api import checkpoint_peek
     path = tmp_path / "c.spdk"
-    fake_checkpoint(path)
+    fake_checkpoint(path, version=version)
     info = checkpoint_peek(str(path))
     assert info == {"t": 0.125, "t_output": 0.25, "steps": 17, "outputs": 3, "precision": "fp32", "p": 3,
                     "N": [64, 48, 1], "integrator": 0, "rk_order": 1}
@@ -140,7 +148,8 @@ def test_restore_refuses_another_configuration(tmp_path):
     a = blast(32)
     path = str(tmp_path / "c.spdk")
     a.checkpoint(path)
-    for kw in ({"precision": "fp32"}, {"N": [32, 16, 1]}, {"p": 2}):
+    for kw in ({"precision": "fp32"}, {"N": [32, 16, 1]}, {"p": 2}, {"L": [2.0, 1.0, 1.0]},
+               {"g": [0.0, -0.1, 0.0]}, {"nad_tolerance": 1e-4}, {"sed": False}):
         b = blast(32, **kw)
         with pytest.raises(SpdkError, match="another configuration"):
             b.restore(path)
@@ -175,3 +184,29 @@ def test_driver_restart_reproduces_the_final_output(tmp_path):
     steps_full = int(out1.split("evolution: ")[1].split(" steps")[0])
     steps_part = int(out2.split("evolution: ")[1].split(" steps")[0])
     assert steps_part == steps_full
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dt_out", [None, 0.0007])
+def test_evolve_resumes_a_restored_run(tmp_path, dt_out):
+    """spdk_hydro_evolve_from continues a restored run at the checkpoint's t
+    and next output time: the same steps and state as one uninterrupted
+    device loop."""
+    import spd_k_b200 as S
+    t_mid, t_end = 0.0015, 0.004
+    a = blast(32)
+    a.run(t_mid, dt_out)
+    path = str(tmp_path / "mid.spdk")
+    a.checkpoint(path, t=a.t, t_output=a.t_output or 0.0, steps=a.n_step)
+    b = blast(32)
+    info = b.restore(path)
+    n_b = b.evolve(t_end, dt_out, t0=info["t"], t_output=info["t_output"] if dt_out else None)
+    c = blast(32)
+    n_c = c.evolve(t_end, dt_out)
+    assert a.n_step + n_b == n_c
+    assert b.t == c.t and b.dt() == c.dt()
+    assert same_bits(b.read(S.FIELD_U_SP), c.read(S.FIELD_U_SP))
+    # already past t_end: no step, t stays
+    assert b.evolve(t_end, dt_out, t0=t_end, t_output=t_end) == 0 and b.t == t_end
+    for s in (a, b, c):
+        s.close()
