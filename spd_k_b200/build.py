@@ -22,7 +22,7 @@ SOURCES = ["spdk_hydro.cu", "spdk_select_2d_low.cu", "spdk_select_2d_high.cu", "
            "spdk_batch_f32.cu", "spdk_batch_host.cu", "spdk_checkpoint.cu", "spdk_setup.cpp", "spdk_host_api.cpp"]
 FP32_SOURCES = {"spdk_select_f32_2d.cu", "spdk_select_f32_3d.cu", "spdk_batch_f32.cu"}
 HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_kernelset.cuh", "spdk_setup.h",
-           "spdk_reflayout.cuh", "spdk_learned_impl.h", "spdk_batch.cuh", "spdk_hydro_impl.h", "spdk_viscous.cuh"]
+           "spdk_reflayout.cuh", "spdk_learned_impl.h", "spdk_batch.cuh", "spdk_hydro_impl.h", "spdk_viscous.cuh", "spdk_picard2d.cuh"]
 
 
 def nvcc_path():

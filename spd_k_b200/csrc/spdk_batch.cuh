@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>)
     picard_batched(const BatchItem<PicardArgsT<R>>* __restrict__ items, int n, DevMatsT<R> M) {
     long long b;
     const BatchItem<PicardArgsT<R>>& it = batch_item(items, n, &b);
-    picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(it.G, M, it.A, b);
+    if constexpr (D == 2) picard2d_body<R, P, TX, TY, MODE, false>(it.G, M, it.A, b);
+    else picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(it.G, M, it.A, b);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>

@@ -992,26 +992,38 @@ __device__ __forceinline__ void picard_kernel_body(const DevGrid& G, const DevMa
     }
 }
 
+}  // namespace spdk
+
+#include "spdk_picard2d.cuh"
+
+namespace spdk {
+
 // VISC: instantiation that adds the viscous interface fluxes (hydro/nu > 0);
-// the inviscid kernels carry none of that code
+// the inviscid kernels carry none of that code. 2D runs take the
+// line-organised pass of spdk_picard2d.cuh.
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
 __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
     pdl_wait();
     if (gate_closed(G)) return;
-    picard_kernel_body<R, D, P, TX, TY, TZ, MODE, VISC>(G, M, A, blockIdx.x);
+    if constexpr (D == 2) picard2d_body<R, P, TX, TY, MODE, VISC>(G, M, A, blockIdx.x);
+    else picard_kernel_body<R, D, P, TX, TY, TZ, MODE, VISC>(G, M, A, blockIdx.x);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
 constexpr size_t picard_smem_bytes() {
-    using S = Shape<D, P>;
-    using TL = Tile<D, TX, TY, TZ>;
-    size_t a = 2 * (size_t)TL::NS * PicardPad<D, P, R>::SS;
-    size_t b = (size_t)kFxBuffers<R> * D * TL::NE * S::V * PicardPad<D, P, R>::FXS;
-    size_t c = (size_t)TL::NE * S::V * S::NFP;
-    size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
-    size_t total = a + b + c;
-    if (need_epi > total) total = need_epi;
-    return total * sizeof(R);
+    if constexpr (D == 2) {
+        return Smem2<R, P, TX, TY>::bytes;
+    } else {
+        using S = Shape<D, P>;
+        using TL = Tile<D, TX, TY, TZ>;
+        size_t a = 2 * (size_t)TL::NS * PicardPad<D, P, R>::SS;
+        size_t b = (size_t)kFxBuffers<R> * D * TL::NE * S::V * PicardPad<D, P, R>::FXS;
+        size_t c = (size_t)TL::NE * S::V * S::NFP;
+        size_t need_epi = 2 * (size_t)TL::NE * S::V * S::NPT;  // W_sp + sweep scratch reuse
+        size_t total = a + b + c;
+        if (need_epi > total) total = need_epi;
+        return total * sizeof(R);
+    }
 }
 
 }  // namespace spdk

@@ -23,6 +23,7 @@ def run_form(prec, learned):
     import bench
     import spd_k_b200 as S
     from helpers import gpu_config
+    from spd_k_b200.api import FIELD_ELEMENT_PREDICTED, FIELD_ELEMENT_TROUBLES
     from spd_k_b200.learned import Indicator, set_indicator
     from test_gpu_precision import element_means
     ov = bench.workload_overrides(N) + [f"time/tlim={T_END!r}", f"output/dt={T_END!r}"]
@@ -36,8 +37,8 @@ def run_form(prec, learned):
     m = element_means(s)
     stats = {"steps": s.n_step}
     if learned:
-        stats["predicted_last_step"] = int(s.read(S.FIELD_ELEMENT_PREDICTED).sum())
-        stats["flagged_last_step"] = int(s.read(S.FIELD_ELEMENT_TROUBLES).sum())
+        stats["predicted_last_step"] = int(s.read(FIELD_ELEMENT_PREDICTED).sum())
+        stats["flagged_last_step"] = int(s.read(FIELD_ELEMENT_TROUBLES).sum())
         set_indicator(s, None)
         ind.close()
     s.close()
