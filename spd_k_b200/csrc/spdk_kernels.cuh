@@ -531,10 +531,19 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // In 3D at p = 5 the FP64 passes' 161 KB of shared memory admit one block
 // per SM anyway, so they take the whole register file instead of spilling
 // at 128 registers.
-template <typename R, int D, int P, int MODE>
+// The FP64 3D passes on 2x2x1-element tiles (p = 2, 3) are compiled for one
+// block per SM as well: at p = 3 their 154 KB of shared memory admit only
+// one; at p = 2, compiled for two blocks (128 registers, 300-450 bytes of
+// spills per thread) they gave results that differ from the oracle in every
+// value after one ADER step, while the same source compiled without spills
+// (one block, 188-211 registers) is bit-identical. Extra barriers around the
+// staging and disabling the first-pass shortcut did not change the spilled
+// build's results; the tile index arithmetic was checked against the
+// oracle at p = 1 and p = 3 on the same tiles.
+template <typename R, int D, int P, int MODE, int NE = 1>
 constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
                                        ? (P == 3 ? (MODE == kFlux ? 5 : 4) : 3)
-                                       : (sizeof(R) == 8 && D == 3 && P >= 5)
+                                       : (sizeof(R) == 8 && D == 3 && (P >= 5 || (NE >= 4 && P >= 2)))
                                              ? 1
                                              : (MODE == kFlux && D == 2 && P == 3 ? 3 : 2);
 
@@ -1002,7 +1011,7 @@ namespace spdk {
 // the inviscid kernels carry none of that code. 2D runs take the
 // line-organised pass of spdk_picard2d.cuh.
 template <typename R, int D, int P, int TX, int TY, int TZ, int MODE, bool VISC = false>
-__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
+__global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE, TX * TY * TZ>) picard_kernel(DevGrid G, DevMatsT<R> M, PicardArgsT<R> A) {
     pdl_wait();
     if (gate_closed(G)) return;
     if constexpr (D == 2) picard2d_body<R, P, TX, TY, MODE, VISC>(G, M, A, blockIdx.x);

@@ -181,12 +181,27 @@ bool pick2(int Nx, int Ny, KernelSetT<R>* k, bool visc) {
 }
 // 3D: one element per tile, or 2x1x1 elements at p <= 3, where one
 // element's (p+1)^3 points would leave most of the block idle in the
-// per-point phases
+// per-point phases; the FP64 form takes 2x2x1 elements at p = 2, 3 when
+// nx1 and nx2 are even
 template <typename R, int P>
-bool pick3(int Nx, int, int, KernelSetT<R>* k, bool visc) {
-    if (visc) *k = make_set<R, 3, P, 1, 1, 1, true>();
-    else if (P <= 3 && Nx % 2 == 0) *k = make_set<R, 3, P, 2, 1, 1>();
-    else *k = make_set<R, 3, P, 1, 1, 1>();
+bool pick3(int Nx, int Ny, int, KernelSetT<R>* k, bool visc) {
+    if (visc) {
+        *k = make_set<R, 3, P, 1, 1, 1, true>();
+        return true;
+    }
+    if constexpr (sizeof(R) == 8 && (P == 2 || P == 3)) {
+        if (Nx % 2 == 0 && Ny % 2 == 0) {
+            *k = make_set<R, 3, P, 2, 2, 1>();
+            return true;
+        }
+    }
+    if constexpr (P <= 3) {
+        if (Nx % 2 == 0) {
+            *k = make_set<R, 3, P, 2, 1, 1>();
+            return true;
+        }
+    }
+    *k = make_set<R, 3, P, 1, 1, 1>();
     return true;
 }
 

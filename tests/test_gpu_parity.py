@@ -141,6 +141,14 @@ RANDOM_CASES = {
     "3d_p3_fallback_tile2": ["job/fallback=true", "mesh/nx1=2", "mesh/nx2=3", "mesh/nx3=2", "mesh/x2_bc=reflective"],
     "3d_p2_fallback_tile2": ["job/fallback=true", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=3", "mesh/nx3=2",
                              "mesh/x1_bc=gradfree"],
+    # FP64 tiles of 2x2x1 elements (p = 2, 3, even nx1 and nx2), with and
+    # without the fallback
+    "3d_p2_ader_tile22_423": ["job/fallback=false", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=2", "mesh/nx3=3"],
+    "3d_p2_fallback_tile22_443": ["job/fallback=true", "mesh/p=2", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=3",
+                                  "mesh/x2_bc=reflective"],
+    "3d_p3_fallback_tile22_443": ["job/fallback=true", "mesh/nx1=4", "mesh/nx2=4", "mesh/nx3=3",
+                                  "mesh/x1_bc=gradfree"],
+    "3d_p3_ader_tile22_423": ["job/fallback=false", "mesh/nx1=4", "mesh/nx2=2", "mesh/nx3=3"],
     # viscous terms on every boundary kind, ADER and SSP-RK, with the fallback
     "2d_p3_viscous_fallback_reflective": ["job/fallback=true", "mesh/nx1=6", "mesh/nx2=4", "mesh/nx3=1",
                                           "mesh/x1_bc=reflective", "mesh/x2_bc=gradfree", "hydro/nu=0.02"],
