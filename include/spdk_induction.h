@@ -76,6 +76,68 @@ int spdk_induction_field_size(spdk_induction* s, int field, size_t* count);
 /* blocking copy of a field to host doubles (B2_cv is computed on demand) */
 int spdk_induction_read(spdk_induction* s, int field, double* host, size_t count);
 
+/* ---------------------------------------------------------------------------
+ * 2D induction solver: the field-loop advection of the induction solver on a
+ * plane field B = (B_x, B_y, 0) with a uniform in-plane velocity, where only
+ * the edge EMF E_z is nonzero. No counterpart in the reference as a 2D code
+ * (Induction_ader requires three active directions,
+ * src/induction_ader.hpp:106-110, and fixes v = (1, 1, 0) and the loop centre,
+ * src/induction.cpp:28-31, src/initial_conditions.cpp:235-249): it computes
+ * what a quasi-2D reference run computes (nx3 = 2, periodic z, induction/nu =
+ * 0, the reference's velocity() and magnetic_loop() returning the values
+ * given here), and its FP64 face fields are that run's. Box
+ * [0, L_x] x [0, L_y], periodic; ADER or SSP-RK1/2/3; no fallback (the
+ * reference detects troubles but applies no fallback for B). Same status
+ * codes as spdk.h.
+ * ------------------------------------------------------------------------- */
+typedef struct spdk_induction2d_config {
+    int p;                    /* polynomial degree, 1..7 */
+    int N[2];                 /* elements along x and y (>= 2) */
+    double L[2];              /* box lengths */
+    int integrator;           /* SPDK_INTEGRATOR_ADER / _RK (spdk.h) */
+    int rk_order;             /* 1..3 for RK */
+    double cfl;
+    double velocity[2];       /* uniform advection velocity (v_x, v_y) */
+    double loop_center[2];    /* magnetic loop: A_z = A0 (R - r) for r <= R about the centre */
+    double loop_A0, loop_R;
+    int precision;            /* SPDK_PRECISION_FP64 (reference arithmetic) or _FP32 (FP32 state) */
+    int device;
+} spdk_induction2d_config;
+
+typedef struct spdk_induction2d spdk_induction2d;
+
+typedef struct spdk_induction2d_info {
+    int p, N[2];
+    long long n_elements;
+    long long n_face_values;      /* B_x and B_y values: 2 E (p+1)(p+2) */
+    int n_time_slices;
+    int launches_per_step;
+} spdk_induction2d_info;
+
+enum {
+    SPDK_IND2_FIELD_BX = 0,     /* [element][jj][ix]: (p+1) x (p+2) per element, element = j Nx + i */
+    SPDK_IND2_FIELD_BY = 1,     /* [element][jy][ii]: (p+2) x (p+1) */
+    SPDK_IND2_FIELD_B2_CV = 2   /* [element][4][jj][ii]: the quasi-2D reference run's B2_cv
+                                   (Bx, By, Bz, |B|^2 sub-cell averages) at its z sub-cell row 0 */
+};
+
+int spdk_induction2d_create(const spdk_induction2d_config* cfg, spdk_induction2d** out);
+int spdk_induction2d_destroy(spdk_induction2d* s);
+int spdk_induction2d_get_info(const spdk_induction2d* s, spdk_induction2d_info* info);
+/* the step size of the next step (the reference's Dt unless clamped) */
+int spdk_induction2d_get_dt(spdk_induction2d* s, double* dt);
+int spdk_induction2d_set_dt(spdk_induction2d* s, double dt);
+/* one ADER / SSP-RK step, asynchronous on the solver's stream */
+int spdk_induction2d_step(spdk_induction2d* s);
+int spdk_induction2d_sync(spdk_induction2d* s);
+/* the CUDA stream (cudaStream_t) every launch of the solver is ordered on */
+int spdk_induction2d_get_stream(spdk_induction2d* s, void** stream);
+/* Induction_ader::time_evolution (src/induction_ader.hpp:273-330): steps of
+ * Dt from t = 0 until t >= t_end, clamped to output times when dt_output > 0 */
+int spdk_induction2d_evolve(spdk_induction2d* s, double t_end, double dt_output, long long* steps, double* t);
+/* blocking copy of a field to host doubles */
+int spdk_induction2d_read(spdk_induction2d* s, int field, double* host, size_t count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -155,3 +155,149 @@ class InductionSolver:
         a = np.empty(n.value, dtype=np.float64)
         _check(L, L.spdk_induction_read(self.h, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n.value))
         return a
+
+
+# ---------------------------------------------------------------------------
+# 2D induction solver (include/spdk_induction.h, spdk_induction2d_*)
+# ---------------------------------------------------------------------------
+FIELD2_BX, FIELD2_BY, FIELD2_B2_CV = 0, 1, 2
+
+
+class Induction2DConfig(ctypes.Structure):
+    _fields_ = [
+        ("p", ctypes.c_int), ("N", ctypes.c_int * 2), ("L", ctypes.c_double * 2), ("integrator", ctypes.c_int),
+        ("rk_order", ctypes.c_int), ("cfl", ctypes.c_double), ("velocity", ctypes.c_double * 2),
+        ("loop_center", ctypes.c_double * 2), ("loop_A0", ctypes.c_double), ("loop_R", ctypes.c_double),
+        ("precision", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class Induction2DInfo(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_int), ("N", ctypes.c_int * 2), ("n_elements", ctypes.c_longlong),
+                ("n_face_values", ctypes.c_longlong), ("n_time_slices", ctypes.c_int),
+                ("launches_per_step", ctypes.c_int)]
+
+
+def field_loop_config(N=512, p=4, L=2.0, velocity=(2.0, 1.0), center=(1.0, 1.0), A0=1e-3, R=0.3, cfl=0.8,
+                      integrator="ader", precision="fp64"):
+    """the 2D field-loop advection: [0, L]^2 periodic (the box [-1, 1]^2 shifted
+    by 1 when L = 2 and the centre is (1, 1)), A_z = A0 (R - r) inside r <= R"""
+    return dict(p=p, N=[N, N], L=[L, L], velocity=list(velocity), center=list(center), A0=A0, R=R, cfl=cfl,
+                integrator=integrator, precision=precision)
+
+
+def make_induction2d_config(c, device=0):
+    o = Induction2DConfig()
+    o.p = c["p"]
+    for d in range(2):
+        o.N[d] = c["N"][d]
+        o.L[d] = c["L"][d]
+        o.velocity[d] = c["velocity"][d]
+        o.loop_center[d] = c["center"][d]
+    integ = c.get("integrator", "ader")
+    if integ == "ader":
+        o.integrator, o.rk_order = 0, 3
+    elif integ.startswith("rk") and len(integ) == 3 and integ[2] in "123":
+        o.integrator, o.rk_order = 1, int(integ[2])
+    else:
+        raise ValueError(f"unknown integrator {integ!r} (ader, rk1, rk2, rk3)")
+    o.cfl = c["cfl"]
+    o.loop_A0, o.loop_R = c["A0"], c["R"]
+    prec = c.get("precision", "fp64")
+    if prec not in ("fp64", "fp32"):
+        raise ValueError(f"unknown precision {prec!r}")
+    o.precision = 0 if prec == "fp64" else 1
+    o.device = device
+    return o
+
+
+def _lib2():
+    L = load_library()
+    if not getattr(L, "_induction2d_types", False):
+        vp = ctypes.c_void_p
+        L.spdk_induction2d_create.argtypes = [ctypes.POINTER(Induction2DConfig), ctypes.POINTER(vp)]
+        L.spdk_induction2d_destroy.argtypes = [vp]
+        L.spdk_induction2d_get_info.argtypes = [vp, ctypes.POINTER(Induction2DInfo)]
+        L.spdk_induction2d_get_dt.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.spdk_induction2d_set_dt.argtypes = [vp, ctypes.c_double]
+        L.spdk_induction2d_step.argtypes = [vp]
+        L.spdk_induction2d_sync.argtypes = [vp]
+        L.spdk_induction2d_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+        L.spdk_induction2d_evolve.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_longlong),
+                                              ctypes.POINTER(ctypes.c_double)]
+        L.spdk_induction2d_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t]
+        L._induction2d_types = True
+    return L
+
+
+class Induction2D:
+    """GPU 2D induction solver: field-loop advection with a uniform in-plane
+    velocity (a quasi-2D run of the reference's Induction_ader)."""
+
+    def __init__(self, c, device=0):
+        L = _lib2()
+        self.c = c
+        self._cfg = make_induction2d_config(c, device)
+        h = ctypes.c_void_p()
+        _check(L, L.spdk_induction2d_create(ctypes.byref(self._cfg), ctypes.byref(h)))
+        self.h = h
+        info = Induction2DInfo()
+        _check(L, L.spdk_induction2d_get_info(self.h, ctypes.byref(info)))
+        self.info = info
+        self.p, self.N = c["p"], list(c["N"])
+        self.t = 0.0
+        self.n_step = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib2().spdk_induction2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def dt(self):
+        v = ctypes.c_double()
+        L = _lib2()
+        _check(L, L.spdk_induction2d_get_dt(self.h, ctypes.byref(v)))
+        return v.value
+
+    def step(self):
+        L = _lib2()
+        _check(L, L.spdk_induction2d_step(self.h))
+
+    def sync(self):
+        L = _lib2()
+        _check(L, L.spdk_induction2d_sync(self.h))
+
+    def stream(self):
+        """the cudaStream_t handle the solver launches on"""
+        L = _lib2()
+        sp = ctypes.c_void_p()
+        _check(L, L.spdk_induction2d_get_stream(self.h, ctypes.byref(sp)))
+        return sp.value
+
+    def evolve(self, t_end, dt_output=None):
+        L = _lib2()
+        steps, t = ctypes.c_longlong(), ctypes.c_double()
+        _check(L, L.spdk_induction2d_evolve(self.h, t_end, dt_output or -1.0, ctypes.byref(steps), ctypes.byref(t)))
+        self.n_step += steps.value
+        self.t = t.value
+        return steps.value
+
+    def read(self, field):
+        n, nf, E = self.p + 1, self.p + 2, self.info.n_elements
+        count = E * n * nf if field in (FIELD2_BX, FIELD2_BY) else 4 * E * n * n
+        a = np.empty(count, dtype=np.float64)
+        L = _lib2()
+        _check(L, L.spdk_induction2d_read(self.h, field, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), count))
+        return a
+
+    def b2_cv(self):
+        """(4, Ny, Nx, n, n): Bx, By, Bz, |B|^2 sub-cell averages"""
+        n = self.p + 1
+        a = self.read(FIELD2_B2_CV).reshape(self.N[1], self.N[0], 4, n, n)
+        return np.ascontiguousarray(a.transpose(2, 0, 1, 3, 4))

@@ -11,7 +11,7 @@ overrides of the reference defaults, and stores, per case:
 It also records the SHA-256 of the reference's committed goldens
 (tests/goldens/ in the reference tree) and the induction solver's outputs
 (INDUCTION_CASES). Needs the reference tree; run once:
-    python tests/golden/make_fixtures.py [--induction]
+    python tests/golden/make_fixtures.py [--induction | --viscous | --loop2d]
 """
 import hashlib
 import json
@@ -133,6 +133,49 @@ def induction_fixtures(manifest):
             print(name, last, steps, flush=True)
 
 
+# 2D field-loop advection (the 2D induction solver): quasi-2D runs (nx3 = 2,
+# periodic, B_z = 0) of the reference built with v = (2, 1, 0) and the loop
+# centred at (1, 1) on [0, 2]^2 (oracle/patch_loop2d.py, make -C oracle
+# loop2d); induction/nu = 0 (no resistive dt cap), fallback off
+LOOP2D_BIN = os.path.join(ROOT, "oracle", "_ref", "spd_K_loop2d")
+LOOP2D_BASE = ["job/system=induction", "induction/nu=0", "job/fallback=false", "mesh/x1len=2", "mesh/x2len=2",
+               "mesh/x3len=1", "mesh/nx3=2", "time/cfl=0.8"]
+LOOP2D_CASES = {
+    "loop2d_n16_p4_ader": ["mesh/p=4", "mesh/nx1=16", "mesh/nx2=16", "time/tlim=0.1", "output/dt=0.1"],
+    "loop2d_n12_p3_rk2": ["mesh/p=3", "mesh/nx1=12", "mesh/nx2=12", "time/integrator=rk2", "time/tlim=0.1",
+                          "output/dt=0.1"],
+    "loop2d_n8x12_p2_ader": ["mesh/p=2", "mesh/nx1=8", "mesh/nx2=12", "time/tlim=0.15", "output/dt=0.05"],
+}
+
+
+def loop2d_fixtures(manifest):
+    for name, ov in LOOP2D_CASES.items():
+        ov = LOOP2D_BASE + ov
+        p = int([o for o in ov if o.startswith("mesh/p=")][0].split("=")[1])
+        nx = int([o for o in ov if o.startswith("mesh/nx1=")][0].split("=")[1])
+        ny = int([o for o in ov if o.startswith("mesh/nx2=")][0].split("=")[1])
+        n = p + 1
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out + "/", OMP_NUM_THREADS="8")
+            r = subprocess.run([LOOP2D_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            files = [f for f in os.listdir(out) if f.startswith("B2_cv_")]
+            last = max(files, key=lambda f: int(f.split("_")[-2]))
+            steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            b = np.fromfile(os.path.join(out, last)).reshape(4, 4, ny + 2, nx + 2, n, n, n)
+            act = b[:, 1:3, 1:-1, 1:-1]          # the two active z elements
+            # the run is z-independent: both z elements are equal, and the z
+            # sub-cell rows differ only by the rounding of the z averaging weights
+            assert np.array_equal(act[:, 0], act[:, 1]), name
+            scale = np.abs(act[:, 0]).max()
+            assert all(np.abs(act[:, 0, :, :, 0] - act[:, 0, :, :, kk]).max() <= 1e-13 * scale for kk in range(n)), name
+            np.savez_compressed(os.path.join(HERE, name + ".npz"),
+                                B2_cv=np.ascontiguousarray(act[:, 0, :, :, 0]))
+            manifest.setdefault("loop2d_cases", {})[name] = {
+                "overrides": ov, "output": last, "steps": steps, "sha256_B2_cv": sha256(os.path.join(out, last)),
+                "velocity": [2.0, 1.0], "center": [1.0, 1.0]}
+            print(name, last, steps, flush=True)
+
+
 def sha256(path):
     h = hashlib.sha256()
     with open(path, "rb") as f:
@@ -228,6 +271,13 @@ if __name__ == "__main__":
             m = json.load(f)
         for name, ov in VISCOUS_CASES.items():
             hydro_case(name, ov, m.setdefault("viscous_cases", {}))
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(m, f, indent=1)
+    elif "--loop2d" in sys.argv:
+        # regenerate only the 2D field-loop fixtures, keeping the rest of the manifest
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            m = json.load(f)
+        loop2d_fixtures(m)
         with open(os.path.join(HERE, "manifest.json"), "w") as f:
             json.dump(m, f, indent=1)
     elif "--induction" in sys.argv:
