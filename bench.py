@@ -360,6 +360,48 @@ def mid_run_state(c, t_mid, local):
     return u, t, n
 
 
+def induction2d_leg(args, local, dist):
+    """the 2D field-loop configuration (512^2 elements, p = 4, v = (2, 1),
+    [-1, 1]^2 periodic as [0, 2]^2): graph-free steps of the native 2D
+    induction solver in the plain FP64 and the FP32 form, CUDA events on the
+    solver stream. DOF = elements x (p+1)^2 solution points; the algorithmic
+    HBM bytes of an ADER step are the face fields' compulsory traffic of its
+    fused passes: first pass B in, nt slices out; later passes nt slices + B
+    in, nt slices out; corrector nt slices + B in, B out."""
+    import torch
+    from spd_k_b200.induction import Induction2D, field_loop_config
+    hbm, peak_kind = peaks()
+    out = {"workload": "field loop 2D, 512^2 elements, p=4, v=(2,1), A_z=1e-3 (0.3 - r), periodic, ADER",
+           "unit": "DOF-updates/s"}
+    for prec in ("fp64", "fp32"):
+        c = field_loop_config(N=512, p=4, precision=prec)
+        s = Induction2D(c)
+        st = torch.cuda.ExternalStream(s.stream(), device=f"cuda:{local}")
+        for _ in range(3):
+            s.step()
+        s.sync()
+        barrier(dist)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.induction_steps):
+            s.step()
+        e1.record(st)
+        e1.synchronize()
+        ms = max_over_ranks(dist, e0.elapsed_time(e1), f"cuda:{local}") / args.induction_steps
+        n, nf, nt = c["p"] + 1, c["p"] + 2, c["p"] + 1
+        E = c["N"][0] * c["N"][1]
+        S2 = 2 * E * n * nf * (8 if prec == "fp64" else 4)
+        alg = (S2 + nt * S2) + (nt - 2) * (2 * nt + 1) * S2 + (nt + 2) * S2
+        gbs = alg / (ms * 1e-3) / 1e9
+        out[prec] = {"value": E * n * n / (ms * 1e-3), "ms_per_step": ms, "steps": args.induction_steps,
+                     "launches_per_step": s.info.launches_per_step, "algorithmic_bytes_per_step": alg,
+                     "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                                  "peak_source": peak_kind}}
+        s.close()
+    return out
+
+
 def run_reference_arm(args):
     rank, world, local, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
                                 int(os.environ.get("LOCAL_RANK", "0")), None)
@@ -400,6 +442,8 @@ def main():
     ap.add_argument("--batch-problems", type=int, default=512,
                     help="problems of the batched-ensemble leg (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--induction-steps", type=int, default=20,
+                    help="steps of the 2D field-loop leg (0: skip it)")
     ap.add_argument("--t-mid", type=float, default=0.025,
                     help="simulated time of the state the steps are timed from (0: the initial blast)")
     args = ap.parse_args()
@@ -588,6 +632,9 @@ def main():
     if args.batch_problems > 0:
         batched = batched_leg(args, local, dist, world, rank)
 
+    # ---- 2D field-loop advection (the native 2D induction solver) ----
+    induction2d = induction2d_leg(args, local, dist) if args.induction_steps > 0 else None
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -629,6 +676,7 @@ def main():
             "mixed_without_indicator": mixed,
             "initial_state": initial,
             "batched": batched,
+            "induction2d": induction2d,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -157,9 +157,41 @@ __global__ void __launch_bounds__(256, 3) ind2_pass(Ind2Geo G, Ind2Mats<R> M, In
             Sby[q] = bys[g];
         }
         __syncthreads();
-        // ---- raw E_z at the edge points of every staged element ----
-        for (int q = tid; q < NS * nf * nf; q += 256) {
-            const int sl = q / (nf * nf), ix = q % nf, jy = (q / nf) % nf;
+        // ---- raw E_z at the edge points the tile's sweeps read: every point
+        // of the tile elements; of the ring, the column (row) next to the
+        // tile and the corner point next to it ----
+        constexpr int TXn = TX * nf, TYn = TY * nf;
+        constexpr int NRAW = NE * nf * nf + 2 * TYn + 2 * TXn + 4;
+        for (int q = tid; q < NRAW; q += 256) {
+            int sl, ix, jy;
+            if (q < NE * nf * nf) {
+                const int el = q / (nf * nf);
+                sl = (el / TX + 1) * SX + el % TX + 1;
+                ix = q % nf;
+                jy = (q / nf) % nf;
+            } else {
+                int r = q - NE * nf * nf;
+                if (r < 2 * TYn) {          // left / right ring: the column next to the tile
+                    const int side = r / TYn;
+                    r %= TYn;
+                    sl = (r / nf + 1) * SX + (side ? TX + 1 : 0);
+                    jy = r % nf;
+                    ix = side ? 0 : nf - 1;
+                } else if ((r -= 2 * TYn) < 2 * TXn) {  // bottom / top ring: the row next to the tile
+                    const int side = r / TXn;
+                    r %= TXn;
+                    sl = (side ? TY + 1 : 0) * SX + r / nf + 1;
+                    ix = r % nf;
+                    jy = side ? 0 : nf - 1;
+                } else {                    // the four ring corners: the point next to the tile
+                    r -= 2 * TXn;
+                    const int cx = r & 1, cy = r >> 1;
+                    sl = (cy ? TY + 1 : 0) * SX + (cx ? TX + 1 : 0);
+                    ix = cx ? 0 : nf - 1;
+                    jy = cy ? 0 : nf - 1;
+                }
+            }
+            const int qo = (sl * nf + jy) * nf + ix;
             const R* X = Sbx + sl * FB;  // [jj][ix]
             const R* Y = Sby + sl * FB;  // [jy][ii]
             R b1 = 0, b2 = 0;
@@ -168,7 +200,7 @@ __global__ void __launch_bounds__(256, 3) ind2_pass(Ind2Geo G, Ind2Mats<R> M, In
                 b1 += X[l * nf + ix] * Msf[jy * n + l];
                 b2 += Y[jy * n + l] * Msf[ix * n + l];
             }
-            Er[q] = vx * b2 - vy * b1;
+            Er[qo] = vx * b2 - vy * b1;
         }
         __syncthreads();
         // ---- unique E_z at the tile elements' edge points ----
