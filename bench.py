@@ -249,16 +249,19 @@ def barrier(dist):
         dist.barrier()
 
 
-def batched_configs(count, seed=2024, precision="fp32"):
+def batched_configs(count, seed=2024, precision="fp32", side=(64, 512)):
     """seeded ensemble of four-quadrant Riemann problems: element counts per
-    side uniform in {16, 24, ..., 64}, p uniform in {2, 3, 5}, rho and P in
-    U[0.1, 1], v in U[-1, 1], gamma 1.4, HLLC + NAD/MUSCL fallback, outflow"""
+    side uniform in {side[0], side[0] + 8, ..., side[1]} (the batched
+    configuration's {64..512}; multiples of 8 so every autotuner tile
+    divides them), p uniform in {2, 3, 5}, rho and P in U[0.1, 1], v in
+    U[-1, 1], gamma 1.4, HLLC + NAD/MUSCL fallback, outflow. The first k
+    problems of a seed are the same whatever count is asked for."""
     import numpy as np
     from spd_k_b200.api import apply_overrides, config_from_params
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
-        nx, ny = (int(v) for v in rng.integers(2, 9, 2) * 8)
+        nx, ny = (int(v) for v in rng.integers(side[0] // 8, side[1] // 8 + 1, 2) * 8)
         p = int(rng.choice([2, 3, 5]))
         ov = ["job/fallback=true", f"mesh/p={p}", f"mesh/nx1={nx}", f"mesh/nx2={ny}", "mesh/nx3=1",
               "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "problem/problem=quadrant", "hydro/gamma=1.4",
@@ -285,16 +288,16 @@ def batched_leg(args, local, dist, world, rank=0):
     cfgs = batched_configs(args.batch_problems)
     idx, mine = B.shard(cfgs, rank, world)
     total_dof = sum(B.problem_dof(c) for c in cfgs)
-    ms_local, info = 0.0, None
-    if mine:
-        b = B.Batch(mine, device=local)
-        b.autotune(2)
+
+    def run(configs, tune=True):
+        """(ms per step, launches per step, groups) of one batch of the given problems"""
+        b = B.Batch(configs, device=local)
+        if tune:
+            b.autotune(2)
         info = b.info()
         st = torch.cuda.ExternalStream(b.stream(), device=f"cuda:{local}")
         b.steps(3)
         b.sync()
-    barrier(dist)       # every rank takes the same collective steps, with or without problems
-    if mine:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -302,19 +305,41 @@ def batched_leg(args, local, dist, world, rank=0):
         e1.record(st)
         e1.synchronize()
         b.sync()
-        ms_local = e0.elapsed_time(e1)
-    ms = max_over_ranks(dist, ms_local, f"cuda:{local}")
+        ms = e0.elapsed_time(e1) / args.batch_steps
+        groups = {int(info.group_p[g]): {"problems": int(info.group_size[g]), "tile": int(info.group_tile[g])}
+                  for g in range(info.n_groups)}
+        out = (ms, info.launches_per_step, groups)
+        b.close()
+        return out
+
+    ms_local, lps, groups = 0.0, None, None
+    barrier(dist)       # every rank takes the same collective steps, with or without problems
+    if mine:
+        ms_local, lps, groups = run(mine)
+    ms = max_over_ranks(dist, ms_local * args.batch_steps, f"cuda:{local}")
     res = {"value": total_dof * args.batch_steps / (ms * 1e-3), "unit": "DOF-updates/s",
            "problems": len(cfgs), "dof": total_dof, "steps": args.batch_steps,
            "scaling": "strong (the ensemble split across ranks)" if world > 1 else "strong",
            "problems_on_rank": len(mine), "ms_per_step": ms / args.batch_steps,
-           "workload": "four-quadrant Riemann ensemble, N per side in {16..64} step 8, p in {2,3,5}, FP32 form, "
-                       "ADER + NAD/MUSCL, autotuned tiles, graph-captured step"}
-    if info is not None:
-        res["launches_per_step"] = info.launches_per_step
-        res["groups"] = {int(info.group_p[g]): {"problems": int(info.group_size[g]), "tile": int(info.group_tile[g])}
-                         for g in range(info.n_groups)}
-        b.close()
+           "workload": (f"the first {len(cfgs)} problems of the seeded four-quadrant Riemann ensemble: N per side "
+                        "in {64..512} step 8, p in {2,3,5}, FP32 form, ADER + NAD/MUSCL, autotuned tiles, "
+                        "graph-captured step"),
+           "launches_per_step": lps, "groups": groups}
+    # per order: the same problems batched by order alone, and one problem of
+    # that order at the group's mean size stepped alone
+    if world == 1 and mine and args.batch_groups:
+        per = {}
+        for p in sorted({c["p"] for c in mine}):
+            sub = [c for c in mine if c["p"] == p]
+            dof = sum(B.problem_dof(c) for c in sub)
+            ms_g, _, g = run(sub)
+            side = int(round((sum(c["N"][0] * c["N"][1] for c in sub) / len(sub)) ** 0.5 / 8)) * 8
+            one = dict(sub[0], N=[side, side, 1])
+            ms_1, _, _ = run([one])
+            per[p] = {"problems": len(sub), "dof": dof, "ms_per_step": ms_g, "value": dof * 1e3 / ms_g,
+                      "tile": g[p]["tile"],
+                      "single_problem": {"side": side, "value": B.problem_dof(one) * 1e3 / ms_1}}
+        res["per_order"] = per
     return res
 
 
@@ -402,6 +427,42 @@ def induction2d_leg(args, local, dist):
     return out
 
 
+def tensor_core_study(args, local):
+    """the FP32 Picard pass's divergence contraction for one slice of the
+    blast (N^2 elements x 4 variables, p = 3) on CUDA cores and on tensor
+    cores (3xTF32 mma.sync), CUDA events, average over 20 calls"""
+    import ctypes
+    import torch
+    import spd_k_b200 as S
+    L = S.load_library()
+    f = L.spdk_study_divergence
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_longlong] + [ctypes.c_void_p] * 4
+    count = args.N * args.N * 4
+    dev = torch.device(f"cuda:{local}")
+    g = torch.Generator(device=dev)
+    g.manual_seed(3)
+    fx = torch.randn(count, 4, 5, device=dev, generator=g)
+    fy = torch.randn(count, 4, 5, device=dev, generator=g)
+    out = torch.empty(count, 4, 4, device=dev)
+    st = torch.cuda.current_stream(dev)
+    res = {"element_variables": count, "bytes_per_call": (fx.numel() + fy.numel() + out.numel()) * 4}
+    for mode, name in ((0, "cuda_cores"), (1, "tensor_cores_3xtf32")):
+        for _ in range(3):
+            f(mode, 3, count, fx.data_ptr(), fy.data_ptr(), out.data_ptr(), st.cuda_stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record(st)
+        for _ in range(reps):
+            f(mode, 3, count, fx.data_ptr(), fy.data_ptr(), out.data_ptr(), st.cuda_stream)
+        e1.record(st)
+        e1.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / reps
+        res[name] = {"us": us, "gbs": res["bytes_per_call"] / (us * 1e-6) / 1e9}
+    res["tensor_over_cuda_cores_time"] = res["tensor_cores_3xtf32"]["us"] / res["cuda_cores"]["us"]
+    return res
+
+
 def run_reference_arm(args):
     rank, world, local, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
                                 int(os.environ.get("LOCAL_RANK", "0")), None)
@@ -439,9 +500,13 @@ def main():
     ap.add_argument("--learned", default=DEFAULT_INDICATOR,
                     help="weights of the learned a-priori indicator ('none': without it)")
     ap.add_argument("--threshold", type=float, default=0.5)
-    ap.add_argument("--batch-problems", type=int, default=512,
-                    help="problems of the batched-ensemble leg (0: skip it)")
-    ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-problems", type=int, default=64,
+                    help="problems of the batched-ensemble leg, the first of its seeded ensemble (0: skip it)")
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--batch-groups", type=int, default=1,
+                    help="also time each order's problems as their own batch and one single problem per order")
+    ap.add_argument("--tc-study", type=int, default=1,
+                    help="time the divergence contraction on CUDA cores and on tensor cores (0: skip)")
     ap.add_argument("--induction-steps", type=int, default=20,
                     help="steps of the 2D field-loop leg (0: skip it)")
     ap.add_argument("--t-mid", type=float, default=0.025,
@@ -635,6 +700,9 @@ def main():
     # ---- 2D field-loop advection (the native 2D induction solver) ----
     induction2d = induction2d_leg(args, local, dist) if args.induction_steps > 0 else None
 
+    # ---- the divergence contraction on CUDA cores against tensor cores ----
+    tc_study = tensor_core_study(args, local) if args.tc_study else None
+
     # ---- CPU baseline (rank 0, N=1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -677,6 +745,7 @@ def main():
             "initial_state": initial,
             "batched": batched,
             "induction2d": induction2d,
+            "tensor_core_study": tc_study,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

@@ -266,6 +266,16 @@ int spdk_hydro_step_noalloc(const spdk_hydro_config* cfg, const double* u_in, do
  * counterpart in the reference; allocates nothing. */
 int spdk_hydro_noalloc_status(int* status_out, void* stream);
 
+/* Measurement of the FP32 Picard pass's divergence contraction on CUDA cores
+ * against tensor cores (no counterpart in the reference): for count
+ * element-variables of a 2D p = 3 run, dudt[ev][jj][ii] = sum_ll
+ * fx[ev][jj][ll] D[ii][ll] + fy[ev][ii][ll] D[jj][ll], D = dfp_to_sp; fx, fy
+ * are [count][4][5] and dudt [count][4][4] FP32 device arrays. mode 0: FP32
+ * FMAs (the Picard pass's form); mode 1: mma.sync m16n8k8 TF32 with the
+ * 3xTF32 split and FP32 accumulation. Asynchronous on `stream`. */
+int spdk_study_divergence(int mode, int p, long long count, const float* fx, const float* fy, float* dudt,
+                          void* stream);
+
 #ifdef __cplusplus
 }
 #endif

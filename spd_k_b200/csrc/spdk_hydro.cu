@@ -400,7 +400,11 @@ int spdk_hydro_create(const spdk_hydro_config* cfg, spdk_hydro** out) {
         delete h;
         return fail(SPDK_E_ARG, "no kernel instantiation for this ndim/p");
     }
-    for (int d = 0; d < 3; d++) h->tile[d] = h->ks64.tile[d];
+    // the step kernels' tile (their launch grid): the kernel set of the run's
+    // arithmetic; the FP64 set of an FP32 run only serves the element-local
+    // set-up kernels, and the two sets may choose different tiles
+    for (int d = 0; d < 3; d++)
+        h->tile[d] = h->prec == SPDK_PRECISION_FP32 ? h->ks32.tile[d] : h->ks64.tile[d];
     int rc = cudaSetDevice(c.device) == cudaSuccess ? 0 : fail(SPDK_E_CUDA, "cudaSetDevice failed");
     if (rc) { delete h; return rc; }
     build_matrices(c.p, ader, &h->mats);

@@ -1,27 +1,26 @@
-// Fused Picard pass of 2D runs: line-owned interpolation and a
-// register-blocked flux divergence.
+// Fused Picard pass of 2D runs: balanced interface / interior flux points
+// and a register-blocked flux divergence.
 //
 // Same inputs, outputs and arithmetic as picard_kernel_body (spdk_kernels.cuh),
-// reorganised so that operands are read once into registers:
+// reorganised so that operands are read once:
 //
 // * Phase A (fluxes at the flux points of one slice). Interfaces (both
 //   sides extrapolated, ghost image at a non-periodic edge, LLF) take one
 //   thread each; interior flux points are shared by the remaining threads,
-//   ordered by (direction, flux point) so that a warp's points take their
-//   interpolation coefficients from the same compile-time offsets of the
-//   kernel's parameter space: no shared-memory load is spent on them.
+//   ordered by (direction, flux point) so that a warp's points read the same
+//   interpolation coefficients (one broadcast shared-memory word); x lines
+//   are loaded as 16-byte vectors.
 // * Phase B (divergence at the solution points). A thread owns a BX x BY block
 //   of solution points of one variable of one element, for the whole pass:
 //   every x-flux value it reads serves BX points, every y-flux value BY
-//   points. Items are ordered block-major, so a warp's items share their
-//   block, whose index is dispatched to a compile-time instance: the
-//   derivative coefficients are constant operands as well.
-//   Each point's sum keeps the reference's order (flux points outer,
-//   directions inner: src/transforms.cpp:296-303), so the FP64 plain form
-//   is unchanged bit for bit.
-// * Epilogues. The step-start state U is prefetched into shared memory by
-//   bulk copies when the pass starts; results are assembled in shared memory
-//   and written back with coalesced 16-byte stores.
+//   points; items are ordered block-major, so a warp's derivative
+//   coefficients are broadcast words too. Each point's sum keeps the
+//   reference's order (flux points outer, directions inner:
+//   src/transforms.cpp:296-303), so the FP64 plain form is unchanged bit for
+//   bit.
+// * Epilogues. The step-start state of the tile is staged point-major by
+//   coalesced loads while slice 0 arrives; results are assembled in shared
+//   memory and written back with coalesced 16-byte stores.
 #pragma once
 #include <type_traits>
 
@@ -36,16 +35,12 @@ struct DivBlock2 {
     static constexpr int NB = NBX * NBY;
 };
 
-// interface lines of a TX x TY tile: (faces along d) x (rows or columns) x n
+// interfaces of a TX x TY tile per direction: (faces along d) x (rows or columns) x n
 template <int P, int TX, int TY>
 struct Lines2 {
     static constexpr int n = P + 1;
     static constexpr int L0 = (TX + 1) * TY * n;
     static constexpr int L1 = (TY + 1) * TX * n;
-    // each direction starts on a warp boundary: a warp's lines share d
-    static constexpr int W0 = (L0 + 31) / 32 * 32;
-    static constexpr int W1 = (L1 + 31) / 32 * 32;
-    static constexpr int W = W0 + W1;
 };
 
 // shared-memory layout of the 2D pass (in elements of R): staging buffers,
