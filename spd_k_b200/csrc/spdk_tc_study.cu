@@ -6,8 +6,8 @@
 // with D = dfp_to_sp (n x nf). This is the flux divergence of the Picard
 // passes (src/transforms.cpp:296-303) in the FP32 form. Two kernels compute
 // it from the same global arrays:
-//   mode 0 (CUDA cores): one thread per 2 x 2 point block of one ev, the
-//     form the Picard pass uses (FP32 FMAs);
+//   mode 0 (CUDA cores): the same staging, then one thread per 2 x 2 point
+//     block of one ev, the form the Picard pass uses (FP32 FMAs);
 //   mode 1 (tensor cores): one warp per 16 ev's as batched small GEMMs on
 //     mma.sync m16n8k8 TF32 with FP32 accumulation and the 3xTF32 split
 //     (x = hi + lo; lo*hi + hi*lo + hi*hi): the x term with rows (ev, jj),
@@ -37,10 +37,19 @@ struct StudyMats {
     float D[kN * kNF];  // dfp_to_sp [ii][ll]
 };
 
-// mode 0: thread per (ev, 2 x 2 block); consecutive threads take consecutive
-// ev's of one block
+// mode 0: one warp per 16 ev's, staged in shared memory exactly as mode 1
+// stages them (so both modes read their operands the same way, as the
+// Picard pass reads its flux points from shared memory); each lane then
+// takes two (ev, 2 x 2 block) items -- the Picard pass's thread mapping --
+// and computes them with FP32 FMAs
+constexpr int kEvPerWarp = 16;
+constexpr int kWarps = 8;
+
 __global__ void __launch_bounds__(256) div_cuda_cores(StudyMats M, long long count, const float* __restrict__ fx,
                                                      const float* __restrict__ fy, float* __restrict__ dudt) {
+    __shared__ float sx[kWarps][kEvPerWarp * kN * kNF];
+    __shared__ float sy[kWarps][kEvPerWarp * kN * kNF];
+    __shared__ float so[kWarps][kEvPerWarp * kN * kN];
     // the coefficients are read at lane-dependent offsets: shared memory, not
     // the parameter space
     __shared__ float D[kN * kNF];
@@ -48,31 +57,45 @@ __global__ void __launch_bounds__(256) div_cuda_cores(StudyMats M, long long cou
 #pragma unroll
         for (int q = 0; q < kN * kNF; q++) D[q] = M.D[q];
     __syncthreads();
-    const long long items = count * 4;
-    for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < items;
-         o += (long long)gridDim.x * blockDim.x) {
-        const long long ev = o % count;
-        const int b = (int)(o / count);
-        const int bx0 = (b & 1) * 2, by0 = (b >> 1) * 2;
-        const float* X = fx + ev * kN * kNF;  // [jj][ll]
-        const float* Y = fy + ev * kN * kNF;  // [ii][ll]
-        float dd[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-#pragma unroll
-        for (int ll = 0; ll < kNF; ll++) {
-            const float x0 = X[(by0 + 0) * kNF + ll], x1 = X[(by0 + 1) * kNF + ll];
-            const float y0 = Y[(bx0 + 0) * kNF + ll], y1 = Y[(bx0 + 1) * kNF + ll];
-            const float c0 = D[(bx0 + 0) * kNF + ll], c1 = D[(bx0 + 1) * kNF + ll];
-            const float r0 = D[(by0 + 0) * kNF + ll], r1 = D[(by0 + 1) * kNF + ll];
-            dd[0][0] += x0 * c0 + y0 * r0;
-            dd[0][1] += x0 * c1 + y1 * r0;
-            dd[1][0] += x1 * c0 + y0 * r1;
-            dd[1][1] += x1 * c1 + y1 * r1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long groups = (count + kEvPerWarp - 1) / kEvPerWarp;
+    for (long long grp = (long long)blockIdx.x * kWarps + warp; grp < groups; grp += (long long)gridDim.x * kWarps) {
+        const long long ev0 = grp * kEvPerWarp;
+        const int nev = (int)min((long long)kEvPerWarp, count - ev0);
+        for (int q = lane; q < kEvPerWarp * kN * kNF; q += 32) {
+            const bool ok = q < nev * kN * kNF;
+            sx[warp][q] = ok ? fx[ev0 * kN * kNF + q] : 0.f;
+            sy[warp][q] = ok ? fy[ev0 * kN * kNF + q] : 0.f;
         }
-        float* out = dudt + ev * kN * kN;
+        __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 2; j++)
+        for (int k = 0; k < 2; k++) {
+            const int item = lane + 32 * k;  // (block, ev): block-major, 16 ev's per block
+            const int ev = item % kEvPerWarp, b = item / kEvPerWarp;
+            const int bx0 = (b & 1) * 2, by0 = (b >> 1) * 2;
+            const float* X = sx[warp] + ev * kN * kNF;  // [jj][ll]
+            const float* Y = sy[warp] + ev * kN * kNF;  // [ii][ll]
+            float dd[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
 #pragma unroll
-            for (int i = 0; i < 2; i++) out[(by0 + j) * kN + bx0 + i] = dd[j][i];
+            for (int ll = 0; ll < kNF; ll++) {
+                const float x0 = X[(by0 + 0) * kNF + ll], x1 = X[(by0 + 1) * kNF + ll];
+                const float y0 = Y[(bx0 + 0) * kNF + ll], y1 = Y[(bx0 + 1) * kNF + ll];
+                const float c0 = D[(bx0 + 0) * kNF + ll], c1 = D[(bx0 + 1) * kNF + ll];
+                const float r0 = D[(by0 + 0) * kNF + ll], r1 = D[(by0 + 1) * kNF + ll];
+                dd[0][0] += x0 * c0 + y0 * r0;
+                dd[0][1] += x0 * c1 + y1 * r0;
+                dd[1][0] += x1 * c0 + y0 * r1;
+                dd[1][1] += x1 * c1 + y1 * r1;
+            }
+            float* out = so[warp] + ev * kN * kN;
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int i = 0; i < 2; i++) out[(by0 + j) * kN + bx0 + i] = dd[j][i];
+        }
+        __syncwarp();
+        for (int q = lane; q < nev * kN * kN; q += 32) dudt[ev0 * kN * kN + q] = so[warp][q];
+        __syncwarp();
     }
 }
 
@@ -103,8 +126,6 @@ __device__ __forceinline__ void mma_3xtf32(float (&c)[4], const uint32_t (&ah)[4
 
 // mode 1: one warp per 16 ev's; the warp's Fx, Fy rows are staged in shared
 // memory, the two GEMMs' results summed there and written back coalesced
-constexpr int kEvPerWarp = 16;
-constexpr int kWarps = 8;
 
 __global__ void __launch_bounds__(256) div_tensor_cores(StudyMats M, long long count, const float* __restrict__ fx,
                                                        const float* __restrict__ fy, float* __restrict__ dudt) {
@@ -201,15 +222,10 @@ extern "C" int spdk_study_divergence(int mode, int p, long long count, const flo
     StudyMats M;
     for (int q = 0; q < kN * kNF; q++) M.D[q] = (float)m.dfp_to_sp[q];
     cudaStream_t s = (cudaStream_t)stream;
-    if (mode == 0) {
-        const long long items = count * 4;
-        const unsigned blocks = (unsigned)std::min<long long>((items + 255) / 256, 148LL * 32);
-        div_cuda_cores<<<blocks, 256, 0, s>>>(M, count, fx, fy, dudt);
-    } else {
-        const long long groups = (count + kEvPerWarp - 1) / kEvPerWarp;
-        const unsigned blocks = (unsigned)std::min<long long>((groups + kWarps - 1) / kWarps, 148LL * 32);
-        div_tensor_cores<<<blocks, 256, 0, s>>>(M, count, fx, fy, dudt);
-    }
+    const long long groups = (count + kEvPerWarp - 1) / kEvPerWarp;
+    const unsigned blocks = (unsigned)std::min<long long>((groups + kWarps - 1) / kWarps, 148LL * 32);
+    if (mode == 0) div_cuda_cores<<<blocks, 256, 0, s>>>(M, count, fx, fy, dudt);
+    else div_tensor_cores<<<blocks, 256, 0, s>>>(M, count, fx, fy, dudt);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("divergence study: ") + cudaGetErrorString(e));
     return 0;
