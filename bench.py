@@ -49,13 +49,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def workload_overrides(N=256, p=3):
-    return [
-        "job/system=hydro", "job/fallback=true", f"mesh/p={p}", f"mesh/nx1={N}", f"mesh/nx2={N}",
-        "mesh/nx3=1", "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "time/cfl=0.8",
-        "time/integrator=ader", "hydro/gamma=1.4", "problem/problem=spherical_blast",
-        "problem/d0=1.0", f"problem/p0={P0_BLAST!r}", "problem/p1=1e-5", "problem/radius=0.01",
-        "fallback/tolerance=1e-5", "output/dt=-1",
-    ]
+    from spd_k_b200.workloads import blast_overrides
+    return blast_overrides(N, p, 2)
 
 
 def workload_config(N=256, p=3):
@@ -250,30 +245,10 @@ def barrier(dist):
 
 
 def batched_configs(count, seed=2024, precision="fp32", side=(64, 512)):
-    """seeded ensemble of four-quadrant Riemann problems: element counts per
-    side uniform in {side[0], side[0] + 8, ..., side[1]} (the batched
-    configuration's {64..512}; multiples of 8 so every autotuner tile
-    divides them), p uniform in {2, 3, 5}, rho and P in U[0.1, 1], v in
-    U[-1, 1], gamma 1.4, HLLC + NAD/MUSCL fallback, outflow. The first k
-    problems of a seed are the same whatever count is asked for."""
-    import numpy as np
-    from spd_k_b200.api import apply_overrides, config_from_params
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(count):
-        nx, ny = (int(v) for v in rng.integers(side[0] // 8, side[1] // 8 + 1, 2) * 8)
-        p = int(rng.choice([2, 3, 5]))
-        ov = ["job/fallback=true", f"mesh/p={p}", f"mesh/nx1={nx}", f"mesh/nx2={ny}", "mesh/nx3=1",
-              "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "problem/problem=quadrant", "hydro/gamma=1.4",
-              "output/dt=-1"]
-        c = config_from_params(apply_overrides({}, ov))
-        q = []
-        for _ in range(4):
-            q += [rng.uniform(0.1, 1.0), rng.uniform(0.1, 1.0), rng.uniform(-1, 1), rng.uniform(-1, 1)]
-        c["q"] = q
-        c["precision"] = precision
-        out.append(c)
-    return out
+    """the seeded four-quadrant Riemann ensemble of the batched configuration
+    (spd_k_b200.workloads.riemann_ensemble)"""
+    from spd_k_b200.workloads import riemann_ensemble
+    return riemann_ensemble(count, seed, precision, side)
 
 
 def batched_leg(args, local, dist, world, rank=0):

@@ -42,11 +42,13 @@ typedef struct spdk_induction_config {
     int device;
     /* apply a fallback where the corrector detects troubles (no reference
      * counterpart: the reference detects and stops there). Each slice's
-     * edges touching a troubled sub-cell take the first-order upwind EMF of
-     * the slice-start face averages instead of the high-order one, and the
-     * faces are updated again from the edges (constrained transport: the
-     * discrete divergence is unchanged). 0 = the reference's behaviour.
-     * Needs fallback = 1. */
+     * candidate face update is judged by the detector as in the reference;
+     * then the edges touching a troubled sub-cell take the first-order
+     * upwind EMF of the slice-start face averages instead of the high-order
+     * one, and the slice-start faces are updated again from the edges
+     * (constrained transport: the discrete divergence is unchanged).
+     * Bit-identical to the reference built with that step added to its
+     * corrector. 0 = the reference's behaviour. Needs fallback = 1. */
     int fallback_apply;
 } spdk_induction_config;
 

@@ -519,7 +519,7 @@ struct spdk_induction {
     double* bcbuf = nullptr;
     unsigned long long* bcwin = nullptr;  // last-writer claims of the FV ghost fill
     unsigned epoch = 0;
-    SDa Bfp[3], Bader[3], B0[3], Ecc[3], Bcv[3], Tfp[3], B2;
+    SDa Bfp[3], Bader[3], B0[3], Ecc[3], Bcv[3], Bsave[3], Tfp[3], B2;
     FVa Bold[3], Bnew[3], Bo4, Bn4, troubles, alpha[3], Efv[3];
 };
 
@@ -653,20 +653,27 @@ int fv_update(spdk_induction* s) {
         for (int d = 0; d < 3; d++)
             k_edge_integral<<<blocks_for(s->Ecc[d].pts() * 2), kBlock, 0, st>>>(s->Ecc[d], s->Efv[d], s->sp_to_cv,
                                                                                s->n, t, d);
-        // with the fallback applied, this update only forms B_new and
-        // B_old for the detection; the faces are written after the EMFs of
+        // with the fallback applied, the slice-start faces are kept: the
+        // candidate update below is what the detection judges, and the
+        // faces are updated again from the kept ones once the EMFs of
         // troubled edges are replaced
-        const int apply = s->cfg.fallback_apply ? 1 : 0;
-        auto face_update = [&](int write) {
+        const bool apply = s->cfg.fallback_apply != 0;
+        auto face_update = [&]() {
             for (int d = 0; d < 3; d++) {
                 const int e1 = (d + 1) % 3, e2 = (d + 2) % 3;
                 const int dim1 = (d + 1) % 3, dim2 = (d + 2) % 3;
                 k_fv_update_B<<<blocks_for(s->Bcv[d].pts()), kBlock, 0, st>>>(s->Bnew[d], s->Bold[d], s->Bcv[d],
                                                                              s->Efv[e1], s->Efv[e2], s->fvf[dim1],
-                                                                             s->fvf[dim2], s->wt, s->dt, t, d, write);
+                                                                             s->fvf[dim2], s->wt, s->dt, t, d, 1);
             }
         };
-        face_update(apply ? 0 : 1);
+        auto copy_faces = [&](SDa* dst, SDa* src) {
+            for (int d = 0; d < 3; d++)
+                cudaMemcpyAsync(dst[d].p, src[d].p, (size_t)src[d].pts() * sizeof(double), cudaMemcpyDeviceToDevice,
+                                st);
+        };
+        if (apply) copy_faces(s->Bsave, s->Bcv);
+        face_update();
         k_B_cv_from_cf<<<blocks_for(s->Bcv[0].pts()), kBlock, 0, st>>>(s->Bn4, s->Bcv[0], s->Bcv[1], s->Bcv[2],
                                                                        s->fp_to_cv, s->nf);
         // apply_fv_boundaries (:614-643)
@@ -684,8 +691,9 @@ int fv_update(spdk_induction* s) {
         k_ind_relax<<<blocks_for(U.cells()), kBlock, 0, st>>>(s->troubles, s->alpha[0], s->alpha[1], s->alpha[2], mask,
                                                               use_sed ? 1 : 0);
         if (apply) {
-            // upwind EMFs on the troubled edges (slice-start faces, ghosts
-            // filled above), then the face update from the blended edges
+            // upwind EMFs on the troubled edges (slice-start FV faces, ghosts
+            // filled above), then the face update of the kept slice-start
+            // faces from the blended edges
             for (int d = 0; d < 3; d++) {
                 const int dim1 = (d + 1) % 3, dim2 = (d + 2) % 3;
                 const long long edges = (long long)s->Efv[d].cells();
@@ -693,7 +701,8 @@ int fv_update(spdk_induction* s) {
                                                                         s->troubles, d, s->fvn[0], s->fvn[1],
                                                                         s->fvn[2]);
             }
-            face_update(1);
+            copy_faces(s->Bcv, s->Bsave);
+            face_update();
         }
     }
     // Transform_to_sp
@@ -798,6 +807,7 @@ int spdk_induction_create(const spdk_induction_config* cfg, spdk_induction** out
         if (!rc && c.fallback) {
             rc = make_sd(s, &s->Bcv[d], 1, 1, ez, ey, ex);
             if (!rc) rc = make_sd(s, &s->Tfp[d], 1, 1, ez, ey, ex);
+            if (!rc && c.fallback_apply) rc = make_sd(s, &s->Bsave[d], 1, 1, ez, ey, ex);
             if (!rc) rc = make_fv(s, &s->Bold[d], 1, d == 2, d == 1, d == 0);
             if (!rc) rc = make_fv(s, &s->Bnew[d], 1, d == 2, d == 1, d == 0);
             if (!rc) rc = make_fv(s, &s->Efv[d], 1, d != 2, d != 1, d != 0);

@@ -11,7 +11,7 @@ overrides of the reference defaults, and stores, per case:
 It also records the SHA-256 of the reference's committed goldens
 (tests/goldens/ in the reference tree) and the induction solver's outputs
 (INDUCTION_CASES). Needs the reference tree; run once:
-    python tests/golden/make_fixtures.py [--induction | --viscous | --loop2d]
+    python tests/golden/make_fixtures.py [--induction | --viscous | --loop2d | --indfb]
 """
 import hashlib
 import json
@@ -130,6 +130,43 @@ def induction_fixtures(manifest):
                     arrays["troubles"] = np.fromfile(os.path.join(out, tr[0]))
                 np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             manifest.setdefault("induction_cases", {})[name] = entry
+            print(name, last, steps, flush=True)
+
+
+# the applied induction fallback (upwind EMFs on the edges of troubled
+# sub-cells, no reference counterpart): the reference with that step added
+# to its corrector (oracle/patch_indfb.py, make -C oracle indfb); the GPU
+# runs the same decks with fallback/apply=true
+INDFB_BIN = os.path.join(ROOT, "oracle", "_ref", "spd_K_indfb")
+INDFB_CASES = {
+    "indfb_n8_p3_ader": INDUCTION_CASES["ind_golden_n8"],
+    "indfb_n6_p3_rk2": INDUCTION_CASES["ind_n6_p3_rk2_fv"],
+    "indfb_n8_p2_ader": ["job/fallback=true", "mesh/p=2", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=8",
+                         "time/tlim=0.1", "output/dt=0.05"],
+    "indfb_n8_p4_rk3": ["job/fallback=true", "mesh/p=4", "mesh/nx1=8", "mesh/nx2=8", "mesh/nx3=8",
+                        "time/integrator=rk3", "time/tlim=0.05", "output/dt=0.05"],
+}
+# (like the plain reference, the patched build crashes in the FV ghost fill
+# at N = 6 for p = 2 and 4; these are decks it completes)
+
+
+def indfb_fixtures(manifest):
+    for name, ov in INDFB_CASES.items():
+        ov = INDUCTION_BASE + ov
+        with tempfile.TemporaryDirectory() as out:
+            env = dict(os.environ, SPD_OUTPUT_DIR=out + "/", OMP_NUM_THREADS="8")
+            r = subprocess.run([INDFB_BIN] + ov, capture_output=True, text=True, env=env, check=True)
+            files = [f for f in os.listdir(out) if f.startswith("B2_cv_")]
+            last = max(files, key=lambda f: int(f.split("_")[-2]))
+            idx = int(last.split("_")[-2])
+            steps = int(r.stdout.split("evolution: ")[1].split(" steps")[0])
+            tr = [f for f in os.listdir(out) if f.startswith("troubles_") and int(f.split("_")[-2]) == idx][0]
+            troubles = np.fromfile(os.path.join(out, tr))
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), B2_cv=np.fromfile(os.path.join(out, last)),
+                                troubles=troubles)
+            manifest.setdefault("indfb_cases", {})[name] = {
+                "overrides": ov, "output": last, "steps": steps, "sha256_B2_cv": sha256(os.path.join(out, last)),
+                "troubled_cells": int((troubles.reshape(4, -1)[3] > 0).sum())}
             print(name, last, steps, flush=True)
 
 
@@ -271,6 +308,13 @@ if __name__ == "__main__":
             m = json.load(f)
         for name, ov in VISCOUS_CASES.items():
             hydro_case(name, ov, m.setdefault("viscous_cases", {}))
+        with open(os.path.join(HERE, "manifest.json"), "w") as f:
+            json.dump(m, f, indent=1)
+    elif "--indfb" in sys.argv:
+        # regenerate only the applied induction fallback fixtures
+        with open(os.path.join(HERE, "manifest.json")) as f:
+            m = json.load(f)
+        indfb_fixtures(m)
         with open(os.path.join(HERE, "manifest.json"), "w") as f:
             json.dump(m, f, indent=1)
     elif "--loop2d" in sys.argv:

@@ -95,6 +95,26 @@ def _sd_divergence(g, p, N):
     return float(np.abs(d).max() * h / max(np.abs(bx).max(), np.abs(by).max(), np.abs(bz).max()))
 
 
+@pytest.mark.parametrize("case", sorted(M.get("indfb_cases", {})))
+def test_applied_fallback_matches_patched_reference(case):
+    """fallback/apply against the reference built with the same step added
+    to its corrector (oracle/patch_indfb.py): B2_cv and the trouble flags
+    of the last output bit for bit."""
+    info = M["indfb_cases"][case]
+    out, g = run_case(info["overrides"] + ["fallback/apply=true"])
+    idx = int(info["output"].split("_")[-2])
+    assert g.n_step == info["steps"]
+    ref = np.load(f"tests/golden/{case}.npz")
+    b2, tr = out[idx]["B2_cv"], out[idx]["troubles"]
+    assert b2.shape == ref["B2_cv"].shape and tr.shape == ref["troubles"].shape
+    bad = np.flatnonzero(tr != ref["troubles"])
+    assert bad.size == 0, ("troubles", bad.size, bad[:8])
+    bad = np.flatnonzero(b2 != ref["B2_cv"])
+    assert bad.size == 0, (bad.size, bad[:8], np.abs(b2 - ref["B2_cv"]).max())
+    assert int((tr.reshape(4, -1)[3] > 0).sum()) == info["troubled_cells"] > 0
+    g.close()
+
+
 def test_applied_fallback_keeps_div_b_and_limits_the_loop():
     """fallback/apply (no reference counterpart: the reference only
     detects): upwind EMFs on the edges of troubled sub-cells. Constrained

@@ -80,3 +80,38 @@ def test_oracle_matches_reference_binary_on_unseen_config():
         ref = np.fromfile(os.path.join(out, "W_cv_N6p2_1_0.dat"))
     w, steps, o, full = oracle_run(ov)
     assert reference_file_bytes(full) == ref.tobytes()
+
+
+def test_applied_induction_fallback_fixtures_are_not_the_plain_reference():
+    """The applied-fallback fixtures (the reference with the upwind EMF step
+    added, oracle/patch_indfb.py) flag troubles and differ from the plain
+    reference on the same decks, so they pin the added step."""
+    cases = M["indfb_cases"]
+    plain = {"indfb_n8_p3_ader": "ind_golden_n8", "indfb_n6_p3_rk2": "ind_n6_p3_rk2_fv"}
+    for name, info in cases.items():
+        assert info["troubled_cells"] > 0
+        if name in plain:
+            other = M["induction_cases"][plain[name]]
+            assert info["overrides"] == other["overrides"]
+            assert info["sha256_B2_cv"] != other["sha256_B2_cv"]
+    a = np.load(os.path.join(GOLDEN, "indfb_n6_p3_rk2.npz"))["B2_cv"]
+    b = np.load(os.path.join(GOLDEN, "ind_n6_p3_rk2_fv.npz"))["B2_cv"]
+    assert a.shape == b.shape and not np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(os.environ.get("SPDK_REFERENCE_ROOT", "/root/reference"), "src")),
+                    reason="reference tree not present")
+def test_applied_fallback_patch_recipe_applies():
+    """oracle/patch_indfb.py finds each text it patches exactly once."""
+    import importlib.util
+    src = os.path.join(os.environ.get("SPDK_REFERENCE_ROOT", "/root/reference"), "src")
+    spec = importlib.util.spec_from_file_location(
+        "patch_indfb", os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "patch_indfb.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    with tempfile.TemporaryDirectory() as out:
+        mod.main(src, out)
+        text = open(os.path.join(out, "induction_ader.hpp")).read()
+        assert text.count("spdk_apply_fallback(ader, X_dim, Y_dim, Z_dim);") == 1
+        assert text.count("spdk_save_faces();") == 1
+        assert sorted(os.listdir(out)) == ["induction_ader.hpp", "main.cpp", "spd_k.hpp"]
