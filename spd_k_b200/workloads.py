@@ -85,7 +85,7 @@ def hydro_config(name, N, p, precision):
               "problem/problem=kh_noise"]
     elif name == "viscous2d":
         ov = ["job/fallback=true", f"mesh/p={p}", f"mesh/nx1={N}", f"mesh/nx2={N}", "mesh/nx3=1",
-              "problem/problem=kh", "hydro/nu=0.02"]
+              "problem/problem=kelvin_helmholtz", "hydro/nu=0.02"]
     else:
         raise ValueError(name)
     c = config_from_params(apply_overrides({}, ov))
@@ -114,12 +114,16 @@ def run(args):
         N = args.N or {"blast2d": 256, "blast3d": 32, "kh3d": 16, "viscous2d": 128}[name]
         p = args.p or {"kh3d": 5}.get(name, 3)
         g = HydroSolver(hydro_config(name, N, p, args.precision))
+        ind = None
         if args.learned:
             from spd_k_b200.learned import Indicator, set_indicator
-            set_indicator(g, Indicator.load(args.learned), 0.5)
+            ind = Indicator.load(args.learned)  # outlives the solver that uses it
+            set_indicator(g, ind, 0.5)
         g.step()
         ms = _timed(g.step, steps)
         g.close()
+        if ind is not None:
+            ind.close()
         desc = f"{name} N={N} p={p} {args.precision}" + (" learned" if args.learned else "")
     elif name == "batched":
         from spd_k_b200.batch import Batch
