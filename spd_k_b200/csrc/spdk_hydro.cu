@@ -115,7 +115,7 @@ int enqueue_step_t(spdk_hydro* h, const KernelSetT<R>& k, const DevMatsT<R>& dm)
             V.vg[d] = (R*)h->vg[d];
             A.vg[d] = (const R*)h->vg[d];
         }
-        const dim3 grid((unsigned)h->E, (unsigned)(A.in_slices > 1 ? h->nt : 1));
+        const dim3 grid((unsigned)((h->E + k.visc_epb - 1) / k.visc_epb), (unsigned)(A.in_slices > 1 ? h->nt : 1));
         prof_begin(h);
         SPDK_CUDA(launch_pdl(k.visc, grid, dim3(kViscThreads), 0, h->stream, h->G, dm, V));
         prof_end(h, SPDK_KERNEL_OTHER);

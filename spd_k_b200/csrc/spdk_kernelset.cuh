@@ -142,6 +142,7 @@ struct KernelSetT {
     void (*visc)(DevGrid, DevMatsT<R>, ViscArgsT<R>) = nullptr;
     size_t picard_smem = 0, update_smem = 0;
     int tile[3] = {1, 1, 1};
+    int visc_epb = 1;  // elements per block of the viscous face kernel
 };
 using KernelSet = KernelSetT<double>;
 
@@ -156,6 +157,7 @@ KernelSetT<R> make_set() {
     k.init = init_state_kernel<R, D, P>;
     k.derive = derive_kernel<R, D, P>;
     k.visc = visc_face_kernel<R, D, P>;
+    k.visc_epb = ViscShape<R, D, P>::EPB;
     k.picard_smem = picard_smem_bytes<R, D, P, TX, TY, TZ>();
     k.update_smem = UpdateSmem<R, D, P, TX, TY, TZ>::bytes;
     k.tile[0] = TX;

@@ -36,39 +36,61 @@ struct ViscArgsT {
     R* vg[3];        // [slice][E][2][V][NTP] per direction
 };
 
-// one block per (element, slice): blockIdx.x = element, blockIdx.y = slice
+// elements per block: a block owns EPB consecutive elements of one slice,
+// so its threads share the few face, gradient and flux items of each
+// element (one element per block left most of them idle at barriers); as
+// many as fit in 40 KB of shared memory, at most 8
+template <typename R, int D, int P>
+struct ViscShape {
+    using S = Shape<D, P>;
+    static constexpr int n = S::n, nf = S::nf, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
+    static constexpr int SOWN = (D + 1) * NPT, UFP = D * D * NFP, WST = D * 2 * (D + 1) * NTP, DU = D * D * NPT;
+    static constexpr size_t per_element = (size_t)(SOWN + UFP + WST + DU) * sizeof(R);
+    static constexpr int fit = (int)(40960 / per_element);
+    static constexpr int EPB = fit < 1 ? 1 : (fit > 8 ? 8 : fit);
+};
+
+// blockIdx.x = group of EPB elements, blockIdx.y = slice
 template <typename R, int D, int P>
 __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevMatsT<R> M, ViscArgsT<R> A) {
     using S = Shape<D, P>;
+    using VS = ViscShape<R, D, P>;
     constexpr int n = S::n, nf = S::nf, V = S::V, NPT = S::NPT, NTP = S::NTP, NFP = S::NFP;
-    __shared__ R Sown[(D + 1) * NPT];          // rho and momenta of the element
-    __shared__ R Ufp[D * D * NFP];             // [d][momentum][flux point of d]
-    __shared__ R Wst[D * 2 * (D + 1) * NTP];   // [d][side][rho, momenta][tp] interface states
-    __shared__ R dU[D * D * NPT];              // [e][momentum][point] gradients
+    constexpr int EPB = VS::EPB;
+    __shared__ R Sown[EPB][VS::SOWN];   // rho and momenta of each element
+    __shared__ R Ufp[EPB][VS::UFP];     // [d][momentum][flux point of d]
+    __shared__ R Wst[EPB][VS::WST];     // [d][side][rho, momenta][tp] interface states
+    __shared__ R dU[EPB][VS::DU];       // [e][momentum][point] gradients
     __shared__ R Msf[nf * n], Mdf[n * nf];
 
     pdl_wait();
     if (gate_closed(G)) return;
     const int tid = threadIdx.x;
-    const long long ge = blockIdx.x;
-    const int t = blockIdx.y;
     const long long E = G.E;
+    const long long ge0 = (long long)blockIdx.x * EPB;
+    const int ne = (int)(E - ge0 < EPB ? E - ge0 : EPB);  // elements of this block
+    const int t = blockIdx.y;
     const R* src = A.ua_in + (A.in_slices > 1 ? (long long)t * E * V * NPT : 0);
     for (int i = tid; i < nf * n; i += kViscThreads) {
         Msf[i] = M.sp_to_fp[i];
         Mdf[i] = M.dfp_to_sp[i];
     }
-    for (int q = tid; q < (D + 1) * NPT; q += kViscThreads) Sown[q] = src[ge * V * NPT + q];
-    int eg[3];
-    eg[0] = (int)(ge % G.N[0]);
-    eg[1] = (int)((ge / G.N[0]) % G.N[1]);
-    eg[2] = (int)(ge / ((long long)G.N[0] * G.N[1]));
+    for (int q = tid; q < ne * VS::SOWN; q += kViscThreads) {
+        const int el = q / VS::SOWN, r = q % VS::SOWN;
+        Sown[el][r] = src[(ge0 + el) * V * NPT + r];
+    }
     __syncthreads();
 
     // ---- interface states of the 2D faces and interior flux points ----
     constexpr int NFACE = D * 2 * NTP;
     constexpr int NINT = D * (nf - 2) * NTP;
-    for (int q = tid; q < NFACE + NINT; q += kViscThreads) {
+    for (int qq = tid; qq < ne * (NFACE + NINT); qq += kViscThreads) {
+        const int el = qq / (NFACE + NINT), q = qq % (NFACE + NINT);
+        const long long ge = ge0 + el;
+        int eg[3];
+        eg[0] = (int)(ge % G.N[0]);
+        eg[1] = (int)((ge / G.N[0]) % G.N[1]);
+        eg[2] = (int)(ge / ((long long)G.N[0] * G.N[1]));
         int c[3] = {0, 0, 0};
         if (q < NFACE) {
             const int d = q / (2 * NTP), s = (q / NTP) % 2, tp = q % NTP;
@@ -79,7 +101,7 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
                 R a = 0;
                 for (int l = 0; l < n; l++) {
                     c[d] = l;
-                    a += Sown[v * NPT + pt_index<n>(c)] * Msf[row * n + l];
+                    a += Sown[el][v * NPT + pt_index<n>(c)] * Msf[row * n + l];
                 }
                 own[v] = a;
             }
@@ -113,8 +135,8 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
             for (int v = 0; v <= D; v++) {
                 const R uL = s ? own[v] : nb[v], uR = s ? nb[v] : own[v];
                 const R m = wind_mix(uL, uR, R(0.5));
-                Wst[((d * 2 + s) * (D + 1) + v) * NTP + tp] = m;
-                if (v >= 1) Ufp[(d * D + v - 1) * NFP + fi] = m;
+                Wst[el][((d * 2 + s) * (D + 1) + v) * NTP + tp] = m;
+                if (v >= 1) Ufp[el][(d * D + v - 1) * NFP + fi] = m;
             }
         } else {
             const int r = q - NFACE;
@@ -126,19 +148,20 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
                 R a = 0;
                 for (int l = 0; l < n; l++) {
                     c[d] = l;
-                    a += Sown[(1 + m) * NPT + pt_index<n>(c)] * Msf[ll * n + l];
+                    a += Sown[el][(1 + m) * NPT + pt_index<n>(c)] * Msf[ll * n + l];
                 }
                 u[m] = a;
             }
             c[d] = ll;
             const int fi = fp_index<n, nf>(d, c);
-            for (int m = 0; m < D; m++) Ufp[(d * D + m) * NFP + fi] = u[m];
+            for (int m = 0; m < D; m++) Ufp[el][(d * D + m) * NFP + fi] = u[m];
         }
     }
     __syncthreads();
 
     // ---- momentum gradients at the solution points (compute_gradient) ----
-    for (int q = tid; q < D * D * NPT; q += kViscThreads) {
+    for (int qq = tid; qq < ne * D * D * NPT; qq += kViscThreads) {
+        const int el = qq / (D * D * NPT), q = qq % (D * D * NPT);
         const int e = q / (D * NPT), m = (q / NPT) % D, pt = q % NPT;
         int c[3];
         pt_coords<n>(pt, c);
@@ -146,15 +169,17 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
         R du = 0;
         for (int ll = 0; ll < nf; ll++) {
             c[e] = ll;
-            du += div_h(Ufp[(e * D + m) * NFP + fp_index<n, nf>(e, c)] * Mdf[id * nf + ll], (R)G.h[e], (R)G.rh[e],
-                        G.pow2[e] != 0);
+            du += div_h(Ufp[el][(e * D + m) * NFP + fp_index<n, nf>(e, c)] * Mdf[id * nf + ll], (R)G.h[e],
+                        (R)G.rh[e], G.pow2[e] != 0);
         }
-        dU[q] = du;
+        dU[el][q] = du;
     }
     __syncthreads();
 
     // ---- viscous fluxes at the face flux points (compute_viscous_flux) ----
-    for (int q = tid; q < NFACE; q += kViscThreads) {
+    for (int qq = tid; qq < ne * NFACE; qq += kViscThreads) {
+        const int el = qq / NFACE, q = qq % NFACE;
+        const long long ge = ge0 + el;
         const int d = q / (2 * NTP), s = (q / NTP) % 2, tp = q % NTP;
         int c[3] = {0, 0, 0};
         tp_coords<D, n>(d, tp, c);
@@ -168,16 +193,16 @@ __global__ void __launch_bounds__(kViscThreads) visc_face_kernel(DevGrid G, DevM
                     c[d] = l;
                     const int pt = pt_index<n>(c);
                     const R mm = Msf[id * n + l];
-                    g1 += dU[(d * D + a) * NPT + pt] * mm;
-                    if (d2 < D) g2 += dU[(d2 * D + a) * NPT + pt] * mm;
-                    if (d3 < D) g3 += dU[(d3 * D + a) * NPT + pt] * mm;
+                    g1 += dU[el][(d * D + a) * NPT + pt] * mm;
+                    if (d2 < D) g2 += dU[el][(d2 * D + a) * NPT + pt] * mm;
+                    if (d3 < D) g3 += dU[el][(d3 * D + a) * NPT + pt] * mm;
                 }
             }
             du1[a] = g1;
             du2[a] = g2;
             du3[a] = g3;
         }
-        const R* ws = Wst + (d * 2 + s) * (D + 1) * NTP + tp;
+        const R* ws = Wst[el] + (d * 2 + s) * (D + 1) * NTP + tp;
         for (int a = 0; a < 3; a++) w[a] = a < D ? ws[(1 + a) * NTP] / ws[0] : R(0);
         R fm[3], fe;
         viscous_flux(du1, du2, du3, w, d, d2, d3, (R)G.nu, (R)G.beta, fm, fe);
