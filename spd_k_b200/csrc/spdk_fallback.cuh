@@ -160,6 +160,18 @@ static __device__ __noinline__ double sed_alpha_staged_2d(const SedGeom S, const
     return smin(m0, sed_component(S, staged, a, 1, k));
 }
 
+// the same for a 3D cell, candidates staged on the tile + 3 halo (rows of
+// E3x, planes of E3x * E3y, origin o - 3)
+static __device__ __noinline__ double sed_alpha_staged_3d(const SedGeom S, const double2* Rn, int E3x, int E3y,
+                                                         const int o[3], const int a[3], int k) {
+    auto staged = [&](const int b[3], int kk) {
+        return rp_var(Rn[(b[0] - o[0] + 3) + E3x * ((b[1] - o[1] + 3) + E3y * (b[2] - o[2] + 3))], kk);
+    };
+    const double m0 = sed_component(S, staged, a, 0, k);
+    const double m1 = smin(m0, sed_component(S, staged, a, 1, k));
+    return smin(m1, sed_component(S, staged, a, 2, k));
+}
+
 // every alpha of the 2D tile + 1 halo (E1x x E1y positions from ox - 1,
 // oy - 1) of the variables in kmask, by the whole block: Al[(k * 2 + d) *
 // E1x * E1y + position]; for blocks with many flagged cells, whose
@@ -184,9 +196,17 @@ static __device__ __noinline__ void sed_al_tile_2d(const SedGeom S, const double
 // so a block waits for one memory round trip, not two. In 2D the kernel is
 // compiled for 4 resident blocks (64 registers, the NAD pass unspilled;
 // measured on B200: 38.6 us against 43.2 us at 6 blocks with spills); in
-// 3D, whose SED reads global memory, without a cap.
+// 3D without a cap.
 template <int D>
 constexpr int kDetectBlocksPerSM = D == 2 ? 4 : 1;
+// 3D tiles whose candidates on the tile + 3 halo fit the static shared
+// memory beside W_old's tile + 1 halo stage them for the SED stencils
+// (a flagged cell otherwise reads its 45 candidates per variable from
+// global memory); the larger ones keep the global reads
+template <int D, int P, int TX, int TY, int TZ>
+constexpr bool kSedStage3 =
+    D == 3 && ((size_t)(TX * (P + 1) + 6) * (TY * (P + 1) + 6) * (TZ * (P + 1) + 6) +
+               (size_t)(TX * (P + 1) + 2) * (TY * (P + 1) + 2) * (TZ * (P + 1) + 2)) * sizeof(double2) <= 46 * 1024;
 // flagged threads of a block above which it evaluates every alpha of its
 // tile once instead of each flagged cell evaluating its own six
 constexpr int kSedTileThreshold = 24;
@@ -202,9 +222,10 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
     constexpr int NC = Bx * By * Bz;
     constexpr int CPT = (NC + kThreads - 1) / kThreads;  // cells per thread
     static_assert(CPT <= 16, "NAD flag bits");
-    constexpr int E3x = Bx + 6, E3y = By + 6;
+    constexpr int E3x = Bx + 6, E3y = By + 6, E3z = D == 3 ? Bz + 6 : 1;
+    constexpr bool stage3 = kSedStage3<D, P, TX, TY, TZ>;
     __shared__ double2 Ro[E1x * E1y * E1z];
-    __shared__ double2 Rn[D == 2 ? E3x * E3y : 1];
+    __shared__ double2 Rn[D == 2 ? E3x * E3y : (stage3 ? E3x * E3y * E3z : 1)];
     __shared__ double Al[D == 2 ? 4 * E1x * E1y : 1];
     const int dz = D == 3 ? 1 : 0;
     int o[3];
@@ -275,18 +296,20 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
             if (un > mx || un < mn) nad |= 1u << (2 * r + k);
         }
     }
-    // SED relaxation of the NAD flags (it can only clear one). In 2D the
-    // block stages the candidates of the tile + 3 halo once when any of its
-    // cells needs it, so a flagged cell reads its stencils from shared
-    // memory instead of a chain of global loads.
+    // SED relaxation of the NAD flags (it can only clear one). In 2D, and
+    // in 3D where it fits, the block stages the candidates of the tile + 3
+    // halo once when any of its cells needs it, so a flagged cell reads its
+    // stencils from shared memory instead of a chain of global loads.
     const int nflag = G.use_sed ? __syncthreads_count(nad != 0) : 0;
     if (nflag) {
-        if (D == 2) {
-            for (int q = threadIdx.x; q < E3x * E3y; q += blockDim.x) {
-                int a[3] = {o[0] - 3 + q % E3x, o[1] - 3 + q / E3x, 0};
+        if (D == 2 || stage3) {
+            for (int q = threadIdx.x; q < E3x * E3y * E3z; q += blockDim.x) {
+                int a[3] = {o[0] - 3 + q % E3x, o[1] - 3 + (q / E3x) % E3y, o[2] - 3 * dz + q / (E3x * E3y)};
                 // three cells outside a non-periodic boundary: never read
-                const bool outside = (G.bc[0] != kPeriodic && (a[0] < -2 || a[0] >= G.N[0] * n + 2)) ||
-                                     (G.bc[1] != kPeriodic && (a[1] < -2 || a[1] >= G.N[1] * n + 2));
+                bool outside = false;
+#pragma unroll
+                for (int d = 0; d < D; d++)
+                    outside |= G.bc[d] != kPeriodic && (a[d] < -2 || a[d] >= G.N[d] * n + 2);
                 bool fl[3];
                 Rn[q] = outside ? make_double2(0.0, 0.0) : rpn[cell_image<D, P>(G, a, fl)];
             }
@@ -324,6 +347,8 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
                     alpha = smin(m0, m1);
                 } else if (D == 2) {
                     alpha = sed_alpha_staged_2d(SG, Rn, E3x, o[0], o[1], a[0], a[1], k);
+                } else if (stage3) {
+                    alpha = sed_alpha_staged_3d(SG, Rn, E3x, E3y, o, a, k);
                 } else {
 #pragma unroll
                     for (int d = 0; d < D; d++) {

@@ -526,8 +526,10 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // the extra resident warps outweigh a few spilled registers (measured on
 // B200: 159 us against 178 us per predictor pass at 256^2). The flux pass
 // keeps no per-slice registers and takes one block more at p = 3 in 2D
-// (FP32 5 blocks: 159 against 167 us; FP64 3 blocks: 338 against 376 us);
-// the predictor and corrector spill heavily there.
+// (FP32 5 blocks: 159 against 167 us; FP64 3 blocks: 338 against 376 us).
+// The FP64 2D predictor and corrector at p = 3 take 3 blocks too (80
+// registers, 184 / 88 bytes of spills): 1.704 against 1.717 ms per plain
+// FP64 step at 256^2.
 // In 3D at p = 5 the FP64 passes' 161 KB of shared memory admit one block
 // per SM anyway, so they take the whole register file instead of spilling
 // at 128 registers.
@@ -545,7 +547,7 @@ constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
                                        ? (P == 3 ? (MODE == kFlux ? 5 : 4) : 3)
                                        : (sizeof(R) == 8 && D == 3 && (P >= 5 || (NE >= 4 && P >= 2)))
                                              ? 1
-                                             : (MODE == kFlux && D == 2 && P == 3 ? 3 : 2);
+                                             : (D == 2 && P == 3 ? 3 : 2);
 
 // flux-point buffers of a Picard pass (alternated between slices when 2)
 template <typename R>
