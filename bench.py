@@ -287,10 +287,31 @@ def batched_leg(args, local, dist, world, rank=0):
         b.close()
         return out
 
+    # an ensemble larger than the device holds runs in waves of at most
+    # batch_wave_dof DOF, one after the other; the step time is their sum
+    waves = [mine] if mine else []
+    if mine and args.batch_wave_dof > 0:
+        waves, cur, cur_dof = [], [], 0
+        for c in mine:
+            d = B.problem_dof(c)
+            if cur and cur_dof + d > args.batch_wave_dof:
+                waves.append(cur)
+                cur, cur_dof = [], 0
+            cur.append(c)
+            cur_dof += d
+        if cur:
+            waves.append(cur)
     ms_local, lps, groups = 0.0, None, None
     barrier(dist)       # every rank takes the same collective steps, with or without problems
-    if mine:
-        ms_local, lps, groups = run(mine)
+    for w in waves:
+        ms_w, lps, g = run(w)
+        ms_local += ms_w
+        groups = groups or {}
+        for p, v in g.items():
+            if p in groups:
+                groups[p]["problems"] += v["problems"]   # the tile reported is the first wave's
+            else:
+                groups[p] = dict(v)
     ms = max_over_ranks(dist, ms_local * args.batch_steps, f"cuda:{local}")
     res = {"value": total_dof * args.batch_steps / (ms * 1e-3), "unit": "DOF-updates/s",
            "problems": len(cfgs), "dof": total_dof, "steps": args.batch_steps,
@@ -299,10 +320,10 @@ def batched_leg(args, local, dist, world, rank=0):
            "workload": (f"the first {len(cfgs)} problems of the seeded four-quadrant Riemann ensemble: N per side "
                         "in {64..512} step 8, p in {2,3,5}, FP32 form, ADER + NAD/MUSCL, autotuned tiles, "
                         "graph-captured step"),
-           "launches_per_step": lps, "groups": groups}
+           "launches_per_step": lps, "groups": groups, "waves": len(waves)}
     # per order: the same problems batched by order alone, and one problem of
     # that order at the group's mean size stepped alone
-    if world == 1 and mine and args.batch_groups:
+    if world == 1 and mine and args.batch_groups and len(waves) == 1:
         per = {}
         for p in sorted({c["p"] for c in mine}):
             sub = [c for c in mine if c["p"] == p]
@@ -478,6 +499,8 @@ def main():
     ap.add_argument("--batch-problems", type=int, default=64,
                     help="problems of the batched-ensemble leg, the first of its seeded ensemble (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--batch-wave-dof", type=float, default=0,
+                    help="run the ensemble in waves of at most this many DOF (0: one batch)")
     ap.add_argument("--batch-groups", type=int, default=1,
                     help="also time each order's problems as their own batch and one single problem per order")
     ap.add_argument("--tc-study", type=int, default=1,

@@ -522,14 +522,15 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 
 // resident blocks per SM the register allocation is sized for: 2 (128
 // registers a thread); for the FP32 form in 2D, whose per-point slices take
-// half the registers of FP64, 3 (85) at p <= 2 and 4 (64) at p = 3, where
+// half the registers of FP64, 3 (85) at p <= 2 and 5 (48) at p = 3, where
 // the extra resident warps outweigh a few spilled registers (measured on
-// B200: 159 us against 178 us per predictor pass at 256^2). The flux pass
-// keeps no per-slice registers and takes one block more at p = 3 in 2D
-// (FP32 5 blocks: 159 against 167 us; FP64 3 blocks: 338 against 376 us).
-// The FP64 2D predictor and corrector at p = 3 take 3 blocks too (80
-// registers, 184 / 88 bytes of spills): 1.704 against 1.717 ms per plain
-// FP64 step at 256^2.
+// B200: 159 us against 178 us per predictor pass at 256^2 going from 2 to
+// 4 blocks; from 4 to 5 blocks, 16 / 8 bytes of spills in the predictor /
+// corrector, 0.798 against 0.812 ms per FP32 blast step at 256^2). The
+// flux pass keeps no per-slice registers (FP32 5 blocks: 159 against 167
+// us; FP64 3 blocks: 338 against 376 us). The FP64 2D predictor and
+// corrector at p = 3 take 3 blocks too (80 registers, 184 / 88 bytes of
+// spills): 1.704 against 1.717 ms per plain FP64 step at 256^2.
 // In 3D at p = 5 the FP64 passes' 161 KB of shared memory admit one block
 // per SM anyway, so they take the whole register file instead of spilling
 // at 128 registers.
@@ -544,7 +545,7 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // oracle at p = 1 and p = 3 on the same tiles.
 template <typename R, int D, int P, int MODE, int NE = 1>
 constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
-                                       ? (P == 3 ? (MODE == kFlux ? 5 : 4) : 3)
+                                       ? (P == 3 ? 5 : 3)
                                        : (sizeof(R) == 8 && D == 3 && (P >= 5 || (NE >= 4 && P >= 2)))
                                              ? 1
                                              : (D == 2 && P == 3 ? 3 : 2);
