@@ -15,7 +15,7 @@
  * largest candidate tile that divides all of the group (tiles 1x1, 2x2 and,
  * for p <= 3, 4x4), all problems in one precision, fallback on or off for
  * all, no learned indicator. Results are bit-identical to stepping each
- * problem alone with spdk_hydro_step.
+ * problem alone with spdk_hydro_step (labels included).
  */
 #ifndef SPDK_BATCH_H
 #define SPDK_BATCH_H
@@ -51,6 +51,12 @@ int spdk_batch_steps(spdk_batch* b, int nsteps);
 int spdk_batch_sync(spdk_batch* b);
 int spdk_batch_get_info(spdk_batch* b, spdk_batch_info* info);
 int spdk_batch_get_stream(spdk_batch* b, void** stream);
+/* on = 1: every replayed step also writes each problem's per-element trouble
+ * labels (1 where NAD/SED/PAD flagged any sub-cell of the element in any
+ * slice of the step), read per member with spdk_hydro_read(
+ * SPDK_FIELD_ELEMENT_TROUBLES) after spdk_batch_sync: the indicator's
+ * training data from the batched run. Needs fallback = 1; blocking. */
+int spdk_batch_record_labels(spdk_batch* b, int on);
 /* the solver of problem i, for spdk_hydro_read / _get_dt after spdk_batch_sync
  * (owned by the batch: do not destroy or step it) */
 int spdk_batch_member(spdk_batch* b, int i, spdk_hydro** h);

@@ -24,6 +24,7 @@ def _lib():
         L.spdk_batch_get_info.argtypes = [vp, ctypes.POINTER(BatchInfo)]
         L.spdk_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
         L.spdk_batch_member.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+        L.spdk_batch_record_labels.argtypes = [vp, ctypes.c_int]
         L._batch_types = True
     return L
 
@@ -113,6 +114,12 @@ class Batch:
         s = ctypes.c_void_p()
         _check(L, L.spdk_batch_get_stream(self.h, ctypes.byref(s)))
         return s.value
+
+    def record_labels(self, on=True):
+        """every replayed step also writes each member's per-element trouble
+        labels (read with member(i).read(FIELD_ELEMENT_TROUBLES))"""
+        L = _lib()
+        _check(L, L.spdk_batch_record_labels(self.h, 1 if on else 0))
 
     def member(self, i):
         """a read-only solver view of problem i (read after sync())"""

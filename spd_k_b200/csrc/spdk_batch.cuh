@@ -61,15 +61,26 @@ __global__ void __launch_bounds__(kThreads, kPicardBlocksPerSM<R, D, P, MODE>)
     else picard_kernel_body<R, D, P, TX, TY, TZ, MODE>(it.G, M, it.A, b);
 }
 
+// the batched detect and update take one block per SM more than the
+// single-problem kernels (the FP64 update excepted: it would spill 350
+// bytes a thread): the groups' many small members leave the single-problem
+// sizing's occupancy unused (measured on the first 16 problems of the
+// ensemble, FP32: 44.7 -> 43.6 ms per step; the single 256^2 blast is
+// 0.3 % slower with the same sizing, so it keeps its own)
+template <int D>
+constexpr int kDetectBlocksPerSMBatched = D == 2 ? 5 : kDetectBlocksPerSM<D>;
+template <typename R, int D, int P>
+constexpr int kUpdateBlocksPerSMBatched = (D == 2 && sizeof(R) == 4) ? 6 : kUpdateBlocksPerSM<D, P>;
+
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads, kDetectBlocksPerSM<D>) detect_batched(const BatchItem<DetectArgs>* __restrict__ items, int n) {
+__global__ void __launch_bounds__(kThreads, kDetectBlocksPerSMBatched<D>) detect_batched(const BatchItem<DetectArgs>* __restrict__ items, int n) {
     long long b;
     const BatchItem<DetectArgs>& it = batch_item(items, n, &b);
     fv_detect_kernel_body<R, D, P, TX, TY, TZ>(it.G, it.A.rpo, it.A.rpn, it.A.T, nullptr, b);
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D, P>)
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSMBatched<R, D, P>)
     update_batched(const BatchItem<FallbackArgsT<R>>* __restrict__ items, int n, DevMatsT<R> M) {
     long long b;
     const BatchItem<FallbackArgsT<R>>& it = batch_item(items, n, &b);

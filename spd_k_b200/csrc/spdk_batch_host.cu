@@ -65,6 +65,7 @@ struct spdk_batch {
     cudaEvent_t fork = nullptr;
     DtArgs* dt_items = nullptr;
     cudaGraphExec_t graph = nullptr;
+    bool labels = false;  // per-step element trouble labels (spdk_batch_record_labels)
 };
 
 namespace {
@@ -177,6 +178,7 @@ int plan_group(spdk_batch* b, Group& g) {
             spdk_hydro* h = b->probs[g.members[q]];
             const BatchItem<PicardArgsT<R>> bq = base(q);
             det[q].G = bq.G;
+            if (b->labels) det[q].G.elem_trouble = h->elem_trouble;
             det[q].first = bq.first;
             det[q].A = DetectArgs{h->rpo, h->rpn, h->trouble};
             up[q].G = bq.G;
@@ -266,6 +268,8 @@ int launch_group(spdk_batch* b, const Group& g, cudaStream_t st) {
 
 // one step: the groups concurrently on their streams, then every dt
 int enqueue_batch_step(spdk_batch* b) {
+    if (b->labels)
+        for (spdk_hydro* h : b->probs) BCUDA(cudaMemsetAsync(h->elem_trouble, 0, (size_t)h->E, b->stream));
     BCUDA(cudaEventRecord(b->fork, b->stream));
     for (Group& g : b->groups) {
         BCUDA(cudaStreamWaitEvent(g.st, b->fork, 0));
@@ -382,6 +386,19 @@ int spdk_batch_steps(spdk_batch* b, int nsteps) {
         if (e != cudaSuccess) return fail(SPDK_E_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(e));
     }
     for (int s = 0; s < nsteps; s++) BCUDA(cudaGraphLaunch(b->graph, b->stream));
+    return 0;
+}
+
+int spdk_batch_record_labels(spdk_batch* b, int on) {
+    if (!b) return fail(SPDK_E_ARG, "null argument");
+    if (on && !b->fallback) return fail(SPDK_E_STATE, "labels come from the fallback's detection: set fallback = 1");
+    BCUDA(cudaStreamSynchronize(b->stream));
+    b->labels = on != 0;
+    for (Group& g : b->groups) {
+        const int rc = b->prec == SPDK_PRECISION_FP32 ? plan_group<float>(b, g) : plan_group<double>(b, g);
+        if (rc) return rc;
+    }
+    drop_graph(b);
     return 0;
 }
 

@@ -4,11 +4,14 @@
 
 Training data are the solver's own a-posteriori NAD/SED/PAD labels (per
 element, any sub-cell in any slice of the step) paired with the feature
-rows of the state before the step, from two families run by this library:
-the 2D point blast (gamma = 1.4, outflow boundaries, p = 3) at 64^2 and
-128^2, and seeded four-quadrant Riemann problems (rho, P in U[0.1, 1],
-v in U[-1, 1]) at 64^2. Classes are balanced by weight; the network is
-trained with the library's own BF16/FP32 forward and backward kernels.
+rows of the state before the step, from the two configurations the
+indicator serves: the 2D point blast (gamma = 1.4, outflow boundaries,
+p = 3) at 64^2 and 128^2, stepped alone, and the batched run of the seeded
+four-quadrant Riemann ensemble (sides 64..512, rho, P in U[0.1, 1], v in
+U[-1, 1]; its p = 3 members among the first 64 problems, FP32 form, labels
+recorded by the batch itself, spdk_batch_record_labels). Classes are
+balanced by weight; the network is trained with the library's own BF16/FP32
+forward and backward kernels.
 """
 import argparse
 import math
@@ -28,22 +31,6 @@ def blast_overrides(N):
             "problem/p1=1e-5", "problem/radius=0.01", "fallback/tolerance=1e-5", "output/dt=-1"]
 
 
-def quadrant_config(N, seed):
-    """a seeded four-quadrant Riemann problem (quadrant IC: q[4 k .. 4 k + 3]
-    = rho, P, vx, vy of quadrant k)"""
-    from .api import apply_overrides, config_from_params
-    rng = np.random.default_rng(seed)
-    ov = ["job/fallback=true", "mesh/p=3", f"mesh/nx1={N}", f"mesh/nx2={N}", "mesh/nx3=1",
-          "mesh/x1_bc=gradfree", "mesh/x2_bc=gradfree", "problem/problem=quadrant", "hydro/gamma=1.4",
-          "output/dt=-1"]
-    c = config_from_params(apply_overrides({}, ov))
-    q = []
-    for _ in range(4):
-        q += [rng.uniform(0.1, 1.0), rng.uniform(0.1, 1.0), rng.uniform(-1, 1), rng.uniform(-1, 1)]
-    c["q"] = q
-    return c
-
-
 def gather(verbose=True):
     import torch
     from . import HydroSolver
@@ -51,7 +38,6 @@ def gather(verbose=True):
     from .learned import collect
     runs = [(config_from_params(apply_overrides({}, blast_overrides(64))), 200, 1),
             (config_from_params(apply_overrides({}, blast_overrides(128))), 300, 3)]
-    runs += [(quadrant_config(64, s), 120, 2) for s in range(6)]
     xs, ys = [], []
     for c, steps, every in runs:
         g = HydroSolver(c)
@@ -61,7 +47,43 @@ def gather(verbose=True):
         ys.append(y)
         if verbose:
             print(f"{c['problem']} {c['N'][0]}^2: {X.shape[0]} rows, {int(y.sum().item())} troubled", flush=True)
+    X, y = batched_rows(verbose=verbose)
+    xs.append(X)
+    ys.append(y)
     return torch.cat(xs), torch.cat(ys)
+
+
+def batched_rows(count=64, p=3, steps=100, every=25, verbose=True):
+    """(X, y) from the batched run of the ensemble's order-p members among
+    its first `count` problems: feature rows of every member before each
+    `every`-th step and the labels the batched step records"""
+    import torch
+    from .api import FIELD_ELEMENT_TROUBLES
+    from .batch import Batch
+    from .learned import features
+    from .workloads import riemann_ensemble
+    cfgs = [c for c in riemann_ensemble(count, precision="fp32") if c["p"] == p]
+    b = Batch(cfgs)
+    b.record_labels(True)
+    xs, ys = [], []
+    for s in range(steps):
+        take = s % every == 0
+        if take:
+            b.sync()
+            rows = [features(b.member(i)) for i in range(len(cfgs))]
+        b.steps(1)
+        if take:
+            b.sync()
+            for i in range(len(cfgs)):
+                lab = np.asarray(b.member(i).read(FIELD_ELEMENT_TROUBLES), dtype=np.float32)
+                xs.append(rows[i])
+                ys.append(torch.from_numpy(lab).cuda())
+    b.close()
+    X, y = torch.cat(xs), torch.cat(ys)
+    if verbose:
+        print(f"batched ensemble, {len(cfgs)} p={p} problems: {X.shape[0]} rows, {int(y.sum().item())} troubled",
+              flush=True)
+    return X, y
 
 
 def main():

@@ -87,3 +87,41 @@ def test_batch_matches_single_solvers(precision, fallback):
         assert same_bits(b.member(i).read(1), s.read(1)), i
         s.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_batch_labels_match_single_solvers():
+    """spdk_batch_record_labels: each member's per-element trouble labels of
+    the last batched step equal the single solver's for the same step (the
+    indicator's training data taken from the batched run); the state stays
+    bit-identical with labels on."""
+    import spd_k_b200 as S
+    import spd_k_b200.batch as B
+    from spd_k_b200.api import FIELD_ELEMENT_TROUBLES, SpdkError
+    cs = ensemble("fp32", True)
+    b = B.Batch(cs)
+    b.record_labels(True)
+    singles = [S.HydroSolver(c) for c in cs]
+    flagged = 0
+    for step in range(3):
+        b.steps(1)
+        b.sync()
+        for s in singles:
+            s.step()
+            s.sync()
+        for i, s in enumerate(singles):
+            m = b.member(i)
+            lb, ls = np.asarray(m.read(FIELD_ELEMENT_TROUBLES)), np.asarray(s.read(FIELD_ELEMENT_TROUBLES))
+            assert np.array_equal(lb, ls), (step, i)
+            flagged += int(lb.sum())
+            assert same_bits(m.read(0), s.read(0)), (step, i)
+    assert flagged > 0
+    for s in singles:
+        s.close()
+    b.close()
+    with pytest.raises(SpdkError):
+        nb = B.Batch(ensemble("fp64", False)[:2])
+        try:
+            nb.record_labels(True)
+        finally:
+            nb.close()
