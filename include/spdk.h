@@ -173,6 +173,13 @@ int spdk_hydro_profile(spdk_hydro* h, int n, double* ms, long long* launches);
  * SPDK_FIELD_U_SP recomputes W_cv and dt */
 int spdk_hydro_read(spdk_hydro* h, int field, double* host, size_t count);
 int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count);
+/* domain integrals of the conserved variables (rho, m_1..m_D, E; count =
+ * D + 2): the sub-cell averages U_cv (sp_to_cv of U_sp along each
+ * direction) times the sub-cell volumes, summed over the active cells in
+ * FP64 with compensated (Neumaier) summation in a fixed order, in both forms
+ * (the reference's mass diagnostic, src/hydro_ader.hpp:481-497, for every
+ * variable). Ordered after the solver's pending work; blocking. */
+int spdk_hydro_conserved(spdk_hydro* h, double* sums, int count);
 
 /* Domain decomposition (slabs; no counterpart in the reference).
  * spdk_hydro_rows copies element rows [lo, hi) of U_sp along the slab axis

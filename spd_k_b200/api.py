@@ -135,6 +135,7 @@ def load_library(path=LIB_PATH):
     L.spdk_checkpoint_peek.argtypes = [ctypes.c_char_p, ci, ip, ip, ip, ip, ip]
     L.spdk_hydro_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
     L.spdk_hydro_slab_dt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+    L.spdk_hydro_conserved.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     _lib = L
     return L
 
@@ -357,6 +358,12 @@ class HydroSolver:
         self.t = t.value
         self.n_step += steps.value
         return steps.value
+
+    def conserved(self):
+        """FP64 domain integrals of (rho, m_1..m_D, E), compensated sums"""
+        a = np.empty(self.nvar, dtype=np.float64)
+        _check(_lib.spdk_hydro_conserved(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), self.nvar))
+        return a
 
     def read(self, field, out=None):
         cells = self.info.n_elements * self.npt

@@ -19,7 +19,8 @@ LIB = os.path.join(HERE, "libspdk_cuda.so")
 SOURCES = ["spdk_hydro.cu", "spdk_select_2d_low.cu", "spdk_select_2d_high.cu", "spdk_select_3d.cu",
            "spdk_select_f32_2d.cu", "spdk_select_f32_3d.cu",
            "spdk_noalloc.cu", "spdk_proto.cu", "spdk_induction.cu", "spdk_induction2d.cu", "spdk_tc_study.cu", "spdk_mlp.cu", "spdk_batch_f64.cu",
-           "spdk_batch_f32.cu", "spdk_batch_host.cu", "spdk_checkpoint.cu", "spdk_setup.cpp", "spdk_host_api.cpp"]
+           "spdk_batch_f32.cu", "spdk_batch_host.cu", "spdk_checkpoint.cu", "spdk_conserved.cu", "spdk_setup.cpp",
+           "spdk_host_api.cpp"]
 FP32_SOURCES = {"spdk_select_f32_2d.cu", "spdk_select_f32_3d.cu", "spdk_batch_f32.cu", "spdk_tc_study.cu"}
 HEADERS = ["spdk_physics.cuh", "spdk_kernels.cuh", "spdk_fallback.cuh", "spdk_kernelset.cuh", "spdk_setup.h",
            "spdk_reflayout.cuh", "spdk_learned_impl.h", "spdk_batch.cuh", "spdk_hydro_impl.h", "spdk_viscous.cuh", "spdk_picard2d.cuh"]
