@@ -196,9 +196,10 @@ static __device__ __noinline__ void sed_al_tile_2d(const SedGeom S, const double
 // so a block waits for one memory round trip, not two. In 2D the kernel is
 // compiled for 4 resident blocks (64 registers, the NAD pass unspilled;
 // measured on B200: 38.6 us against 43.2 us at 6 blocks with spills); in
-// 3D without a cap.
+// 3D for 3 (80 registers, 20-50 bytes of spills; 90 registers and 2
+// blocks uncapped: KH 16^3 p=5 FP64 step 11.40 -> 11.28 ms at 3).
 template <int D>
-constexpr int kDetectBlocksPerSM = D == 2 ? 4 : 1;
+constexpr int kDetectBlocksPerSM = D == 2 ? 4 : 3;
 // 3D tiles whose candidates on the tile + 3 halo fit the static shared
 // memory beside W_old's tile + 1 halo stage them for the SED stencils
 // (a flagged cell otherwise reads its 45 candidates per variable from
@@ -549,7 +550,10 @@ __device__ __forceinline__ void muscl_cell(const DevGrid& G, const int fa[3], in
 // p = 3: 62.6 against 72.0 us in FP32, 139 against 176 us in FP64). In 3D
 // (one element per block) the 140-register kernel ran one block per SM;
 // measured per step of 4 updates, FP64: 32^3 p=3 6.15 / 3.47 / 2.52 ms at
-// 2 / 3 / 4 blocks, 16^3 p=5 4.13 / 3.65 / 4.05 ms
+// 2 / 3 / 4 blocks, 16^3 p=5 4.13 / 3.65 / 4.05 ms. The FP32 3D update
+// above p = 3 fits 4 blocks without spills (64 registers) and takes them:
+// KH 16^3 p=5 FP32 step 4.91 -> 4.68 ms together with the 3D detection's
+// 3 blocks.
 template <int D, int P>
 constexpr int kUpdateBlocksPerSM = D == 2 ? 5 : (P <= 3 ? 4 : 3);
 
@@ -864,7 +868,7 @@ __device__ __forceinline__ void fv_update_kernel_body(const DevGrid& G, const De
 }
 
 template <typename R, int D, int P, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D, P>) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
+__global__ void __launch_bounds__(kThreads, kUpdateBlocksPerSM<D, P> + (sizeof(R) == 4 && D == 3 && P > 3 ? 1 : 0)) fv_update_kernel(DevGrid G, DevMatsT<R> M, FallbackArgsT<R> A) {
     pdl_wait();
     if (gate_closed(G)) return;
     fv_update_kernel_body<R, D, P, TX, TY, TZ>(G, M, A, blockIdx.x);
