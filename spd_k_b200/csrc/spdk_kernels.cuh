@@ -530,7 +530,11 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // flux pass keeps no per-slice registers (FP32 5 blocks: 159 against 167
 // us; FP64 3 blocks: 338 against 376 us). The FP64 2D predictor and
 // corrector at p = 3 take 3 blocks too (80 registers, 184 / 88 bytes of
-// spills): 1.704 against 1.717 ms per plain FP64 step at 256^2.
+// spills): 1.704 against 1.717 ms per plain FP64 step at 256^2. The FP32
+// 3D passes at p <= 3 (2x1x1 tiles, 23-52 KB of shared memory) take 3
+// blocks (80 registers, at most 52 bytes of spills): steps 7.30 -> 6.42 ms
+// (40^3 p=2 blast), 3.58 -> 3.43 ms (24^3 p=3 KH), 4.63 -> 4.60 ms (32^3
+// p=3 blast).
 // In 3D at p = 5 the FP64 passes' 161 KB of shared memory admit one block
 // per SM anyway, so they take the whole register file instead of spilling
 // at 128 registers.
@@ -548,7 +552,7 @@ constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
                                        ? (P == 3 ? 5 : 3)
                                        : (sizeof(R) == 8 && D == 3 && (P >= 5 || (NE >= 4 && P >= 2)))
                                              ? 1
-                                             : (D == 2 && P == 3 ? 3 : 2);
+                                             : (D == 2 && P == 3 ? 3 : ((sizeof(R) == 4 && D == 3 && P <= 3) ? 3 : 2));
 
 // flux-point buffers of a Picard pass (alternated between slices when 2)
 template <typename R>
