@@ -522,11 +522,15 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 
 // resident blocks per SM the register allocation is sized for: 2 (128
 // registers a thread); for the FP32 form in 2D, whose per-point slices take
-// half the registers of FP64, 3 (85) at p <= 2 and 5 (48) at p = 3, where
+// half the registers of FP64, 4 (64) at p <= 2, 5 (48) at p = 3 and 3 (80)
+// above, where
 // the extra resident warps outweigh a few spilled registers (measured on
 // B200: 159 us against 178 us per predictor pass at 256^2 going from 2 to
 // 4 blocks; from 4 to 5 blocks, 16 / 8 bytes of spills in the predictor /
-// corrector, 0.798 against 0.812 ms per FP32 blast step at 256^2). The
+// corrector, 0.798 against 0.812 ms per FP32 blast step at 256^2; p = 2 at
+// 4 blocks and p = 5 at 3, without spills: blast steps 0.328 -> 0.285 ms
+// at 192^2 p=2, 1.635 -> 1.340 ms at 128^2 p=5, the first 16 problems of
+// the batched ensemble 43.6 -> 37.6 ms). The
 // flux pass keeps no per-slice registers (FP32 5 blocks: 159 against 167
 // us; FP64 3 blocks: 338 against 376 us). The FP64 2D predictor and
 // corrector at p = 3 take 3 blocks too (80 registers, 184 / 88 bytes of
@@ -548,8 +552,8 @@ __device__ __forceinline__ void picard_face_item(const DevGrid& G, const DevMats
 // build's results; the tile index arithmetic was checked against the
 // oracle at p = 1 and p = 3 on the same tiles.
 template <typename R, int D, int P, int MODE, int NE = 1>
-constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2 && P <= 3)
-                                       ? (P == 3 ? 5 : 3)
+constexpr int kPicardBlocksPerSM = (sizeof(R) == 4 && D == 2)
+                                       ? (P == 3 ? 5 : (P == 2 ? 4 : 3))
                                        : (sizeof(R) == 8 && D == 3 && (P >= 5 || (NE >= 4 && P >= 2)))
                                              ? 1
                                              : (D == 2 && P == 3 ? 3 : ((sizeof(R) == 4 && D == 3 && P <= 3) ? 3 : 2));
