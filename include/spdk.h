@@ -178,7 +178,8 @@ int spdk_hydro_write(spdk_hydro* h, int field, const double* host, size_t count)
  * direction) times the sub-cell volumes, summed over the active cells in
  * FP64 with compensated (Neumaier) summation in a fixed order, in both forms
  * (the reference's mass diagnostic, src/hydro_ader.hpp:481-497, for every
- * variable). Ordered after the solver's pending work; blocking. */
+ * variable). Ordered after the solver's pending work; blocking. Slab
+ * solvers (slab_n != 0), whose rows include halo rows, are rejected. */
 int spdk_hydro_conserved(spdk_hydro* h, double* sums, int count);
 
 /* Domain decomposition (slabs; no counterpart in the reference).

@@ -121,6 +121,8 @@ extern "C" int spdk_hydro_conserved(spdk_hydro* h, double* sums, int count) {
     if (!h || !sums) return spdk::fail(SPDK_E_ARG, "null argument");
     if (count != h->V) return spdk::fail(SPDK_E_ARG, "count must be " + std::to_string(h->V));
     if (h->D < 2 || h->n > 8) return spdk::fail(SPDK_E_ARG, "2D or 3D, p <= 7");
+    if (h->cfg.slab_n != 0)
+        return spdk::fail(SPDK_E_ARG, "a slab solver holds halo rows: sum the whole domain's solver instead");
     ConservedArgs A{};
     A.u = h->u;
     A.fp32 = h->prec == SPDK_PRECISION_FP32;

@@ -60,3 +60,13 @@ def test_3d_periodic_run_conserves_every_integral():
     scale = np.maximum(np.abs(s0), 1e-3 * np.abs(s0).max())
     assert (np.abs(s1 - s0) / scale < 1e-13).all(), (s0, s1)
     g.close()
+
+
+def test_slab_solvers_are_rejected():
+    import spd_k_b200 as S
+    from spd_k_b200.api import SpdkError
+    c = gpu_config(SINE + ["mesh/x2_bc=gradfree"])
+    g = S.HydroSolver(dict(c, N=[16, 8, 1], slab_lo=4, slab_n=16))
+    with pytest.raises(SpdkError, match="slab"):
+        g.conserved()
+    g.close()
