@@ -668,8 +668,10 @@ __global__ void __launch_bounds__(32) k_mlp_zero_logit(int n_in, const uint16_t*
 // the solver's a-priori flags from its stored feature rows: the nodal part
 // of each row (columns < 2 NPT, written by the step's last update) and the
 // neighbour part formed here from the element means; one warp per 16
-// elements
-__global__ void __launch_bounds__(kTcWarps * 32) k_indicator_rows_tc(const uint16_t* __restrict__ feat,
+// elements. Compiled for 3 resident blocks (80 registers, 72 bytes of
+// spills; 127 registers and 2 blocks otherwise): the timed blast step with
+// the indicator 0.8372 -> 0.8359 ms.
+__global__ void __launch_bounds__(kTcWarps * 32, 3) k_indicator_rows_tc(const uint16_t* __restrict__ feat,
                                                                      const float2* __restrict__ mean, FeatureGeom F,
                                                                      int n_in, const uint16_t* __restrict__ wbf,
                                                                      const float* __restrict__ z0,
