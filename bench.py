@@ -291,16 +291,7 @@ def batched_leg(args, local, dist, world, rank=0):
     # batch_wave_dof DOF, one after the other; the step time is their sum
     waves = [mine] if mine else []
     if mine and args.batch_wave_dof > 0:
-        waves, cur, cur_dof = [], [], 0
-        for c in mine:
-            d = B.problem_dof(c)
-            if cur and cur_dof + d > args.batch_wave_dof:
-                waves.append(cur)
-                cur, cur_dof = [], 0
-            cur.append(c)
-            cur_dof += d
-        if cur:
-            waves.append(cur)
+        waves = B.waves(mine, args.batch_wave_dof)
     ms_local, lps, groups = 0.0, None, None
     barrier(dist)       # every rank takes the same collective steps, with or without problems
     for w in waves:

@@ -63,6 +63,23 @@ def partition(configs, world):
     return [sorted(p) for p in parts]
 
 
+def waves(configs, max_dof):
+    """consecutive groups of the configurations of at most max_dof DOF each
+    (a single problem larger than max_dof forms a group of its own): an
+    ensemble larger than the device holds runs wave after wave"""
+    out, cur, cur_dof = [], [], 0
+    for c in configs:
+        d = problem_dof(c)
+        if cur and cur_dof + d > max_dof:
+            out.append(cur)
+            cur, cur_dof = [], 0
+        cur.append(c)
+        cur_dof += d
+    if cur:
+        out.append(cur)
+    return out
+
+
 def shard(configs, rank, world):
     """(indices, configurations) of this rank's part of the ensemble"""
     idx = partition(configs, world)[rank]

@@ -72,6 +72,20 @@ def test_ensemble_partition_covers_every_problem_once_and_balances():
     assert B.problem_dof(c) == c["N"][0] * c["N"][1] * n * n
 
 
+def test_ensemble_waves_keep_order_and_bound_each_wave():
+    import bench
+    import spd_k_b200.batch as B
+    cfgs = bench.batched_configs(512)
+    total = sum(B.problem_dof(c) for c in cfgs)
+    ws = B.waves(cfgs, 1.0e8)
+    assert [c for w in ws for c in w] == cfgs                     # every problem once, in order
+    assert all(sum(B.problem_dof(c) for c in w) <= 1.0e8 for w in ws)
+    assert len(ws) >= total / 1.0e8
+    big = dict(cfgs[0], N=[512, 512, 1])
+    assert B.waves([big], 1.0) == [[big]]                         # an oversized problem alone
+    assert B.waves(cfgs, total) == [cfgs]
+
+
 def _shard_rank(rank, world, port, q):
     import torch
     import torch.distributed as dist
