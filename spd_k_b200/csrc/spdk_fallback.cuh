@@ -172,6 +172,25 @@ static __device__ __noinline__ double sed_alpha_staged_3d(const SedGeom S, const
     return smin(m1, sed_component(S, staged, a, 2, k));
 }
 
+// every alpha of variable k that the cells of a 3D tile (Bx x By x Bz from
+// o) take along each direction d: the tile extended by one cell along d
+// only, Al = [d = 0: (Bx + 2) By Bz][d = 1: Bx (By + 2) Bz][d = 2: Bx By
+// (Bz + 2)], each x-fastest; candidates staged on the tile + 3 halo
+static __device__ __noinline__ void sed_al_tile_3d(const SedGeom S, const double2* Rn, int E3x, int E3y,
+                                                   const int o[3], int Bx, int By, int Bz, int k, double* Al) {
+    auto staged = [&](const int b[3], int kk) {
+        return rp_var(Rn[(b[0] - o[0] + 3) + E3x * ((b[1] - o[1] + 3) + E3y * (b[2] - o[2] + 3))], kk);
+    };
+    const int n0 = (Bx + 2) * By * Bz, n1 = Bx * (By + 2) * Bz, n2 = Bx * By * (Bz + 2);
+    for (int w = threadIdx.x; w < n0 + n1 + n2; w += blockDim.x) {
+        const int d = w < n0 ? 0 : (w < n0 + n1 ? 1 : 2);
+        const int r = w - (d == 0 ? 0 : (d == 1 ? n0 : n0 + n1));
+        const int ex = Bx + 2 * (d == 0), ey = By + 2 * (d == 1);
+        const int a[3] = {o[0] + r % ex - (d == 0), o[1] + (r / ex) % ey - (d == 1), o[2] + r / (ex * ey) - (d == 2)};
+        Al[w] = sed_al(S, staged, a, d, k);
+    }
+}
+
 // every alpha of the 2D tile + 1 halo (E1x x E1y positions from ox - 1,
 // oy - 1) of the variables in kmask, by the whole block: Al[(k * 2 + d) *
 // E1x * E1y + position]; for blocks with many flagged cells, whose
@@ -322,42 +341,83 @@ __device__ __forceinline__ void fv_detect_kernel_body(const DevGrid& G, const do
             return rp_var(rpn[cell_image<D, P>(G, b, fl)], k);
         };
         const bool tile = D == 2 && nflag > kSedTileThreshold;
-        if (tile) {
-            const unsigned kmask = (__syncthreads_or(nad & 0x55555555u) ? 1u : 0u) |
-                                   (__syncthreads_or(nad & 0xAAAAAAAAu) ? 2u : 0u);
-            sed_al_tile_2d(SG, Rn, E3x, E1x, E1y, o[0], o[1], kmask, Al);
-            __syncthreads();
-        }
+        const bool tile3 = stage3 && nflag > kSedTileThreshold;
+        if (tile3) {
+            if constexpr (stage3) {
+                // many flagged cells: every alpha of the tile once per
+                // variable, in the W_old tile's storage (free after NAD),
+                // then each flagged cell takes the min of its own and its
+                // neighbours' along each direction, in sed_component's order
+                constexpr int n0 = (Bx + 2) * By * Bz, n1 = Bx * (By + 2) * Bz, n2 = Bx * By * (Bz + 2);
+                static_assert((size_t)(n0 + n1 + n2) * sizeof(double) <= sizeof(Ro), "alphas fit the W_old tile");
+                double* Al3 = reinterpret_cast<double*>(Ro);
 #pragma unroll
-        for (int r = 0; r < CPT; r++) {
-            if (!(nad & (3u << (2 * r)))) continue;
-            const int q = threadIdx.x + r * kThreads;
-            int a[3] = {o[0] + q % Bx, o[1] + (q / Bx) % By, o[2] + q / (Bx * By)};
+                for (int k = 0; k < 2; k++) {
+                    if (!__syncthreads_or(nad & (k == 0 ? 0x55555555u : 0xAAAAAAAAu))) continue;
+                    sed_al_tile_3d(SG, Rn, E3x, E3y, o, Bx, By, Bz, k, Al3);
+                    __syncthreads();
 #pragma unroll
-            for (int k = 0; k < 2; k++) {
-                if (!(nad & (1u << (2 * r + k)))) continue;
-                double alpha = 1;
-                if (tile) {
-                    // the alphas of the cell and its neighbours, in the
-                    // order sed_component takes them
-                    const int x = a[0] - o[0] + 1, y = a[1] - o[1] + 1;
-                    const double* A0 = Al + (k * 2 + 0) * E1x * E1y;
-                    const double* A1 = Al + (k * 2 + 1) * E1x * E1y;
-                    const double m0 = smin(smin(A0[(x - 1) + E1x * y], A0[x + E1x * y]), A0[(x + 1) + E1x * y]);
-                    const double m1 = smin(smin(A1[x + E1x * (y - 1)], A1[x + E1x * y]), A1[x + E1x * (y + 1)]);
-                    alpha = smin(m0, m1);
-                } else if (D == 2) {
-                    alpha = sed_alpha_staged_2d(SG, Rn, E3x, o[0], o[1], a[0], a[1], k);
-                } else if (stage3) {
-                    alpha = sed_alpha_staged_3d(SG, Rn, E3x, E3y, o, a, k);
-                } else {
+                    for (int r = 0; r < CPT; r++) {
+                        if (!(nad & (1u << (2 * r + k)))) continue;
+                        const int q = threadIdx.x + r * kThreads;
+                        const int x = q % Bx, y = (q / Bx) % By, z = q / (Bx * By);
+                        double alpha = 1;
 #pragma unroll
-                    for (int d = 0; d < D; d++) {
-                        const double m3 = sed_component(SG, global, a, d, k);
-                        alpha = d == 0 ? m3 : smin(alpha, m3);
+                        for (int d = 0; d < 3; d++) {
+                            double al[3];
+#pragma unroll
+                            for (int sft = -1; sft <= 1; sft++) {
+                                const int i = d == 0 ? (x + 1 + sft) + (Bx + 2) * (y + By * z)
+                                                     : (d == 1 ? n0 + x + Bx * ((y + 1 + sft) + (By + 2) * z)
+                                                               : n0 + n1 + x + Bx * (y + By * (z + 1 + sft)));
+                                al[sft + 1] = Al3[i];
+                            }
+                            const double m3 = smin(smin(al[0], al[1]), al[2]);
+                            alpha = d == 0 ? m3 : smin(alpha, m3);
+                        }
+                        if (!(alpha < 1)) nad &= ~(1u << (2 * r + k));
                     }
+                    __syncthreads();
                 }
-                if (!(alpha < 1)) nad &= ~(1u << (2 * r + k));
+            }
+        } else {
+            if (tile) {
+                const unsigned kmask = (__syncthreads_or(nad & 0x55555555u) ? 1u : 0u) |
+                                       (__syncthreads_or(nad & 0xAAAAAAAAu) ? 2u : 0u);
+                sed_al_tile_2d(SG, Rn, E3x, E1x, E1y, o[0], o[1], kmask, Al);
+                __syncthreads();
+            }
+#pragma unroll
+            for (int r = 0; r < CPT; r++) {
+                if (!(nad & (3u << (2 * r)))) continue;
+                const int q = threadIdx.x + r * kThreads;
+                int a[3] = {o[0] + q % Bx, o[1] + (q / Bx) % By, o[2] + q / (Bx * By)};
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    if (!(nad & (1u << (2 * r + k)))) continue;
+                    double alpha = 1;
+                    if (tile) {
+                        // the alphas of the cell and its neighbours, in the
+                        // order sed_component takes them
+                        const int x = a[0] - o[0] + 1, y = a[1] - o[1] + 1;
+                        const double* A0 = Al + (k * 2 + 0) * E1x * E1y;
+                        const double* A1 = Al + (k * 2 + 1) * E1x * E1y;
+                        const double m0 = smin(smin(A0[(x - 1) + E1x * y], A0[x + E1x * y]), A0[(x + 1) + E1x * y]);
+                        const double m1 = smin(smin(A1[x + E1x * (y - 1)], A1[x + E1x * y]), A1[x + E1x * (y + 1)]);
+                        alpha = smin(m0, m1);
+                    } else if (D == 2) {
+                        alpha = sed_alpha_staged_2d(SG, Rn, E3x, o[0], o[1], a[0], a[1], k);
+                    } else if (stage3) {
+                        alpha = sed_alpha_staged_3d(SG, Rn, E3x, E3y, o, a, k);
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < D; d++) {
+                            const double m3 = sed_component(SG, global, a, d, k);
+                            alpha = d == 0 ? m3 : smin(alpha, m3);
+                        }
+                    }
+                    if (!(alpha < 1)) nad &= ~(1u << (2 * r + k));
+                }
             }
         }
     }
