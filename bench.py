@@ -21,9 +21,16 @@ indicator are timed beside it on the same workload.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--precision fp32|fp64] [--learned PATH|none]
+                  [--batch-problems P] [--batch-steps S] [--batch-wave-dof D]
 
 N>1 runs N independent replicas (one per GPU, weak scaling); the headline
 time is the max over ranks of CUDA-event time on each solver stream.
+
+Beside the headline the line carries the batched ensemble (by default the
+first 64 of the 512 four-quadrant problems, 20 steps; --batch-problems 512
+--batch-wave-dof 1e8 runs the whole configuration in waves that fit the
+device), the 2D field loop, the divergence-contraction study and the
+reference CPU build's throughput.
 """
 import argparse
 import json
